@@ -1,0 +1,249 @@
+/*
+ * nqpu_b200.h — C ABI of the B200 statevector engine.
+ *
+ * The first block of declarations is the drop-in boundary: the same names,
+ * argument meaning, ownership rules and error codes as the reference's C FFI
+ * (sdk/rust/src/infra/bindings/c_ffi.rs, header text at c_ffi.rs:1480-1620),
+ * so a caller linking against the reference's generated `nqpu_metal.h` can link
+ * this library instead.  Each declaration cites the reference entry point it
+ * replaces.  Amplitudes live in B200 HBM; every call runs hand-written sm_100a
+ * kernels on the state's own CUDA stream.  There is no CPU fallback: when no
+ * CUDA device is usable, creation returns NULL and every other call returns
+ * NQPU_SIMULATION_FAILED.
+ *
+ * The second block holds additions in the same conventions (opaque handles,
+ * NqpuError returns, caller-owned output buffers with explicit lengths): the
+ * complex64 state, the extended gate set, whole-register reductions, the fused
+ * (tensor-core) execution mode, batched execution and the request server.
+ *
+ * Threading: a handle is used by one host thread at a time (the reference's
+ * `&mut` aliasing contract, c_ffi.rs:620-650).  The RNG used by measurement and
+ * sampling is thread-local and seeded by nqpu_set_seed, as in c_ffi.rs:49-66.
+ */
+#ifndef NQPU_B200_H
+#define NQPU_B200_H
+
+#include <stdint.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Types (c_ffi.rs:76-204)                                             */
+/* ------------------------------------------------------------------ */
+
+typedef struct NqpuState NqpuState;       /* c_ffi.rs:76  opaque state      */
+typedef struct NqpuCircuit NqpuCircuit;   /* c_ffi.rs:85  opaque circuit    */
+
+typedef enum {                            /* c_ffi.rs:97-113                */
+    NQPU_OK                = 0,
+    NQPU_INVALID_QUBIT     = 1,
+    NQPU_INVALID_PARAMETER = 2,
+    NQPU_ALLOCATION_FAILED = 3,
+    NQPU_SIMULATION_FAILED = 4,
+    NQPU_NULL_POINTER      = 5,
+    NQPU_INVALID_HANDLE    = 6
+} NqpuError;
+
+typedef struct { double re; double im; } NqpuComplex;          /* c_ffi.rs:121 */
+typedef struct { uint32_t outcome; double probability; } NqpuMeasurement; /* :178 */
+typedef struct {                                                 /* c_ffi.rs:188 */
+    uint32_t num_qubits;
+    uint64_t seed;
+    bool     use_gpu;
+    uint32_t num_threads;
+} NqpuConfig;
+typedef struct { uint32_t major; uint32_t minor; uint32_t patch; } NqpuVersion; /* :197 */
+
+/* ------------------------------------------------------------------ */
+/* State management                                                    */
+/* ------------------------------------------------------------------ */
+
+/* c_ffi.rs:789  complex128 state |0..0>; NULL if n==0, n>30 or no device. */
+NqpuState*  nqpu_state_create(uint32_t num_qubits);
+/* c_ffi.rs:805  NULL-safe. */
+void        nqpu_state_destroy(NqpuState* state);
+/* c_ffi.rs:817  device-to-device deep copy; NULL on NULL input or OOM. */
+NqpuState*  nqpu_state_clone(const NqpuState* state);
+/* c_ffi.rs:836  0 on NULL. */
+uint32_t    nqpu_state_num_qubits(const NqpuState* state);
+/* c_ffi.rs:850  index >= 2^n -> NQPU_INVALID_PARAMETER. */
+NqpuError   nqpu_state_get_amplitude(const NqpuState* state, uint64_t index, NqpuComplex* out);
+/* c_ffi.rs:877  does not renormalise. */
+NqpuError   nqpu_state_set_amplitude(NqpuState* state, uint64_t index, NqpuComplex amp);
+/* c_ffi.rs:900  len must be >= 2^n. */
+NqpuError   nqpu_state_probabilities(const NqpuState* state, double* out, uint64_t len);
+/* c_ffi.rs:929  squared norm (FP64 reduction); -1.0 on NULL. */
+double      nqpu_state_norm(const NqpuState* state);
+/* c_ffi.rs:941 */
+NqpuError   nqpu_state_reset(NqpuState* state);
+
+/* ------------------------------------------------------------------ */
+/* Gate operations (c_ffi.rs:956-1140), one kernel launch per gate     */
+/* ------------------------------------------------------------------ */
+
+NqpuError   nqpu_gate_h(NqpuState* state, uint32_t qubit);           /* c_ffi.rs:995  */
+NqpuError   nqpu_gate_x(NqpuState* state, uint32_t qubit);           /* c_ffi.rs:996  */
+NqpuError   nqpu_gate_y(NqpuState* state, uint32_t qubit);           /* c_ffi.rs:997  */
+NqpuError   nqpu_gate_z(NqpuState* state, uint32_t qubit);           /* c_ffi.rs:998  */
+NqpuError   nqpu_gate_s(NqpuState* state, uint32_t qubit);           /* c_ffi.rs:999  */
+NqpuError   nqpu_gate_t(NqpuState* state, uint32_t qubit);           /* c_ffi.rs:1000 */
+NqpuError   nqpu_gate_rx(NqpuState* state, uint32_t qubit, double angle); /* c_ffi.rs:1002 */
+NqpuError   nqpu_gate_ry(NqpuState* state, uint32_t qubit, double angle); /* c_ffi.rs:1003 */
+NqpuError   nqpu_gate_rz(NqpuState* state, uint32_t qubit, double angle); /* c_ffi.rs:1004 */
+NqpuError   nqpu_gate_cx(NqpuState* state, uint32_t control, uint32_t target); /* c_ffi.rs:1010 */
+NqpuError   nqpu_gate_cz(NqpuState* state, uint32_t control, uint32_t target); /* c_ffi.rs:1032 */
+NqpuError   nqpu_gate_swap(NqpuState* state, uint32_t q1, uint32_t q2);       /* c_ffi.rs:1054 */
+/* c_ffi.rs:1079  row-major [[m00,m01],[m10,m11]]. */
+NqpuError   nqpu_gate_custom_1q(NqpuState* state, uint32_t qubit, const NqpuComplex* matrix);
+/* c_ffi.rs:1111  row-major 4x4; basis |q1 q2>, q1 is the HIGH bit of the sub-index. */
+NqpuError   nqpu_gate_custom_2q(NqpuState* state, uint32_t q1, uint32_t q2, const NqpuComplex* matrix);
+
+/* ------------------------------------------------------------------ */
+/* Measurement (c_ffi.rs:1151-1250)                                    */
+/* ------------------------------------------------------------------ */
+
+/* c_ffi.rs:1151  collapse; r drawn from the thread-local xorshift64*. */
+NqpuError   nqpu_measure(NqpuState* state, uint32_t qubit, NqpuMeasurement* out);
+/* c_ffi.rs:1177  qubits measured 0..n-1 in order. */
+NqpuError   nqpu_measure_all(NqpuState* state, uint32_t* out, uint32_t num_qubits);
+/* c_ffi.rs:1205 */
+NqpuError   nqpu_expectation_z(const NqpuState* state, uint32_t qubit, double* out);
+/* c_ffi.rs:1231  outcome = first i with r < cumsum_i (else 2^n-1). */
+NqpuError   nqpu_sample(const NqpuState* state, uint32_t num_shots, uint64_t* out);
+
+/* ------------------------------------------------------------------ */
+/* Circuit API (c_ffi.rs:1259-1400)                                    */
+/* ------------------------------------------------------------------ */
+
+NqpuCircuit* nqpu_circuit_create(uint32_t num_qubits);            /* c_ffi.rs:1259 */
+void         nqpu_circuit_destroy(NqpuCircuit* circuit);          /* c_ffi.rs:1273 */
+NqpuError    nqpu_circuit_add_h(NqpuCircuit* circuit, uint32_t qubit);                 /* :1283 */
+NqpuError    nqpu_circuit_add_cx(NqpuCircuit* circuit, uint32_t control, uint32_t target); /* :1300 */
+NqpuError    nqpu_circuit_add_rx(NqpuCircuit* circuit, uint32_t qubit, double angle);  /* :1322 */
+/* c_ffi.rs:1346  runs the circuit through the tiled multi-gate pass engine. */
+NqpuError    nqpu_circuit_execute(const NqpuCircuit* circuit, NqpuState* state);
+uint32_t     nqpu_circuit_gate_count(const NqpuCircuit* circuit); /* c_ffi.rs:1372 */
+uint32_t     nqpu_circuit_depth(const NqpuCircuit* circuit);      /* c_ffi.rs:1385 */
+
+/* ------------------------------------------------------------------ */
+/* Utility (c_ffi.rs:1403-1470)                                        */
+/* ------------------------------------------------------------------ */
+
+NqpuVersion  nqpu_version(void);                    /* c_ffi.rs:1403 */
+const char*  nqpu_error_message(NqpuError error);   /* c_ffi.rs:1426 */
+void         nqpu_set_seed(uint64_t seed);          /* c_ffi.rs:1444 */
+void         nqpu_set_num_threads(uint32_t threads);/* c_ffi.rs:1460 accepted, no effect on GPU */
+
+/* ================================================================== */
+/* Additions (same conventions)                                         */
+/* ================================================================== */
+
+typedef enum { NQPU_C128 = 0, NQPU_C64 = 1 } NqpuDtype;
+
+/* Engine modes for nqpu_circuit_execute_ex. */
+typedef enum {
+    NQPU_MODE_TILED   = 0,  /* multi-gate smem/register tiled passes (default)       */
+    NQPU_MODE_PERGATE = 1,  /* one full-state kernel launch per gate (plain per-gate) */
+    NQPU_MODE_FUSED   = 2   /* <=5-qubit fusion, split-TF32 tcgen05 contractions      */
+} NqpuMode;
+
+/* Like nqpu_state_create with a dtype; 1 <= n <= 34 (HBM-bounded). */
+NqpuState*  nqpu_state_create_ex(uint32_t num_qubits, NqpuDtype dtype);
+NqpuDtype   nqpu_state_dtype(const NqpuState* state);
+/* Set the state to the computational basis state |index>. */
+NqpuError   nqpu_state_set_basis(NqpuState* state, uint64_t index);
+/* Copy all 2^n amplitudes to the host as complex128 (len >= 2^n). */
+NqpuError   nqpu_state_get_amplitudes(const NqpuState* state, NqpuComplex* out, uint64_t len);
+/* Load all 2^n amplitudes from the host (rounded to the state's dtype). */
+NqpuError   nqpu_state_set_amplitudes(NqpuState* state, const NqpuComplex* in, uint64_t len);
+/* Block until all work queued on the state's stream has finished. */
+NqpuError   nqpu_state_synchronize(const NqpuState* state);
+
+/* Reference GateOperations coverage (R/lib.rs:617-1735, gates.rs). */
+NqpuError   nqpu_gate_sx(NqpuState* state, uint32_t qubit);
+NqpuError   nqpu_gate_phase(NqpuState* state, uint32_t qubit, double theta);
+NqpuError   nqpu_gate_u3(NqpuState* state, uint32_t qubit, double theta, double phi, double lambda);
+NqpuError   nqpu_gate_cphase(NqpuState* state, uint32_t control, uint32_t target, double phi);
+NqpuError   nqpu_gate_crx(NqpuState* state, uint32_t control, uint32_t target, double theta);
+NqpuError   nqpu_gate_cry(NqpuState* state, uint32_t control, uint32_t target, double theta);
+NqpuError   nqpu_gate_crz(NqpuState* state, uint32_t control, uint32_t target, double theta);
+NqpuError   nqpu_gate_iswap(NqpuState* state, uint32_t q1, uint32_t q2);
+NqpuError   nqpu_gate_rzz(NqpuState* state, uint32_t q1, uint32_t q2, double theta);
+NqpuError   nqpu_gate_rxx(NqpuState* state, uint32_t q1, uint32_t q2, double theta);
+NqpuError   nqpu_gate_ryy(NqpuState* state, uint32_t q1, uint32_t q2, double theta);
+NqpuError   nqpu_gate_toffoli(NqpuState* state, uint32_t c1, uint32_t c2, uint32_t target);
+NqpuError   nqpu_gate_ccz(NqpuState* state, uint32_t q1, uint32_t q2, uint32_t q3);
+NqpuError   nqpu_gate_cswap(NqpuState* state, uint32_t control, uint32_t q1, uint32_t q2);
+/* GateType::CU (gates.rs:542): |0><0| x I + e^{i gamma} |1><1| x U3(theta, phi, lambda). */
+NqpuError   nqpu_gate_cu(NqpuState* state, uint32_t control, uint32_t target, double theta,
+                         double phi, double lambda, double gamma);
+/* GateOperations::u2 convention (R/lib.rs:1536): q_lo is bit 0 of the sub-index. */
+NqpuError   nqpu_gate_u2(NqpuState* state, uint32_t q_lo, uint32_t q_hi, const NqpuComplex* matrix);
+/* R/lib.rs:1705 zero the |1> half of `qubit` and renormalise. */
+NqpuError   nqpu_gate_reset_qubit(NqpuState* state, uint32_t qubit);
+
+/* Whole-register reductions (FP64 accumulation). */
+/* All <Z_i>, i = 0..n-1, in one pass (len >= n). R/lib.rs:407 for every qubit. */
+NqpuError   nqpu_expectation_z_all(const NqpuState* state, double* out, uint32_t len);
+/* R/lib.rs:425 / :444 */
+NqpuError   nqpu_expectation_x(const NqpuState* state, uint32_t qubit, double* out);
+NqpuError   nqpu_expectation_y(const NqpuState* state, uint32_t qubit, double* out);
+/* R/lib.rs:465,518 sum_t coeff_t <P_t>; paulis is num_terms strings of n chars
+ * 'I','X','Y','Z' (character q acts on qubit q), packed back to back. */
+NqpuError   nqpu_expectation_pauli_sum(const NqpuState* state, const char* paulis,
+                                       const double* coeffs, uint32_t num_terms, double* out);
+/* R/lib.rs:388 |<a|b>|^2 in FP64; the two states may differ in dtype. */
+NqpuError   nqpu_fidelity(const NqpuState* a, const NqpuState* b, double* out);
+/* Sampling with caller-supplied uniforms in [0,1): out[s] = first i with u[s] < cumsum_i. */
+NqpuError   nqpu_sample_with_uniforms(const NqpuState* state, const double* uniforms,
+                                      uint32_t num_shots, uint64_t* out);
+/* Scale every amplitude by 1/sqrt(norm) (FP64 norm). */
+NqpuError   nqpu_state_renormalize(NqpuState* state);
+
+/* Extended circuit builder: every gate of GateType (R/core/gates/gates.rs:8-62). */
+NqpuError    nqpu_circuit_add_x(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_y(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_z(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_s(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_t(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_sx(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_ry(NqpuCircuit* c, uint32_t q, double angle);
+NqpuError    nqpu_circuit_add_rz(NqpuCircuit* c, uint32_t q, double angle);
+NqpuError    nqpu_circuit_add_phase(NqpuCircuit* c, uint32_t q, double angle);
+NqpuError    nqpu_circuit_add_u3(NqpuCircuit* c, uint32_t q, double theta, double phi, double lambda);
+NqpuError    nqpu_circuit_add_cz(NqpuCircuit* c, uint32_t q1, uint32_t q2);
+NqpuError    nqpu_circuit_add_swap(NqpuCircuit* c, uint32_t q1, uint32_t q2);
+NqpuError    nqpu_circuit_add_iswap(NqpuCircuit* c, uint32_t q1, uint32_t q2);
+NqpuError    nqpu_circuit_add_cphase(NqpuCircuit* c, uint32_t control, uint32_t target, double phi);
+NqpuError    nqpu_circuit_add_crx(NqpuCircuit* c, uint32_t control, uint32_t target, double theta);
+NqpuError    nqpu_circuit_add_cry(NqpuCircuit* c, uint32_t control, uint32_t target, double theta);
+NqpuError    nqpu_circuit_add_crz(NqpuCircuit* c, uint32_t control, uint32_t target, double theta);
+NqpuError    nqpu_circuit_add_rzz(NqpuCircuit* c, uint32_t q1, uint32_t q2, double theta);
+NqpuError    nqpu_circuit_add_rxx(NqpuCircuit* c, uint32_t q1, uint32_t q2, double theta);
+NqpuError    nqpu_circuit_add_ryy(NqpuCircuit* c, uint32_t q1, uint32_t q2, double theta);
+NqpuError    nqpu_circuit_add_toffoli(NqpuCircuit* c, uint32_t c1, uint32_t c2, uint32_t target);
+NqpuError    nqpu_circuit_add_ccz(NqpuCircuit* c, uint32_t q1, uint32_t q2, uint32_t q3);
+NqpuError    nqpu_circuit_add_cswap(NqpuCircuit* c, uint32_t control, uint32_t q1, uint32_t q2);
+NqpuError    nqpu_circuit_add_cu(NqpuCircuit* c, uint32_t control, uint32_t target, double theta,
+                                 double phi, double lambda, double gamma);
+NqpuError    nqpu_circuit_add_custom_1q(NqpuCircuit* c, uint32_t q, const NqpuComplex* matrix);
+/* nqpu_gate_custom_2q convention: q1 is the HIGH bit of the sub-index. */
+NqpuError    nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uint32_t q2, const NqpuComplex* matrix);
+/* Like nqpu_circuit_create with the 34-qubit engine limit. */
+NqpuCircuit* nqpu_circuit_create_ex(uint32_t num_qubits);
+/* Run with an explicit engine mode. */
+NqpuError    nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode);
+/* Plan statistics of the last execution of `circuit` in `mode` on an n-qubit state:
+ * out[0] = HBM passes (kernel launches over the full state), out[1] = lowered ops,
+ * out[2] = register stages (tiled) or fused unitaries (fused).  len >= 3. */
+NqpuError    nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_t num_qubits,
+                                     NqpuDtype dtype, NqpuMode mode, uint64_t* out, uint32_t len);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* NQPU_B200_H */

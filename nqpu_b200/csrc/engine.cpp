@@ -1,0 +1,315 @@
+// Engine objects: device context, state allocation, reductions glue and the
+// circuit runner (tiled passes / per-gate / fused).
+#include "engine.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include "fused.h"
+#include "kernels.h"
+
+namespace nqpu {
+
+namespace {
+std::once_flag g_dev_once;
+bool g_dev_ok = false;
+int g_sms = 148;
+
+void dev_init() {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    g_dev_ok = false;
+    return;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+    g_dev_ok = false;
+    return;
+  }
+  g_sms = p.multiProcessorCount;
+  g_dev_ok = true;
+}
+}  // namespace
+
+bool device_ready() {
+  std::call_once(g_dev_once, dev_init);
+  return g_dev_ok;
+}
+
+int device_sms() {
+  device_ready();
+  return g_sms;
+}
+
+StateImpl* state_new(uint32_t n, DType dt) {
+  if (!device_ready()) return nullptr;
+  auto* s = new (std::nothrow) StateImpl();
+  if (!s) return nullptr;
+  s->n = n;
+  s->dt = dt;
+  s->bytes = size_t(amp_bytes(dt)) << n;
+  bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaMalloc(&s->amp, s->bytes) == cudaSuccess;
+  ok = ok && cudaMalloc(reinterpret_cast<void**>(&s->scratch), reduce_scratch_bytes(int(n))) == cudaSuccess;
+  ok = ok && cudaMalloc(reinterpret_cast<void**>(&s->d_small), 512 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMallocHost(reinterpret_cast<void**>(&s->h_small), 512 * sizeof(double)) == cudaSuccess;
+  ok = ok && launch_set_basis(dt, s->amp, int(n), 0, s->stream, device_sms()) == cudaSuccess;
+  ok = ok && cudaStreamSynchronize(s->stream) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    state_free(s);
+    return nullptr;
+  }
+  return s;
+}
+
+void state_free(StateImpl* s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->amp) cudaFree(s->amp);
+  if (s->scratch) cudaFree(s->scratch);
+  if (s->d_small) cudaFree(s->d_small);
+  if (s->h_small) cudaFreeHost(s->h_small);
+  if (s->d_uni) cudaFree(s->d_uni);
+  if (s->d_shots) cudaFree(s->d_shots);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+cudaError_t state_zsums(const StateImpl* s, double* zs, double* total) {
+  const int n = int(s->n);
+  cudaError_t e = launch_zsums(s->dt, s->amp, n, s->scratch, s->d_small, s->stream, device_sms());
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(s->h_small, s->d_small, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost, s->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return e;
+  if (zs) std::memcpy(zs, s->h_small, sizeof(double) * (n + 1));
+  if (total) *total = s->h_small[0];
+  return cudaSuccess;
+}
+
+cudaError_t state_pauli(const StateImpl* s, uint64_t xm, uint64_t zm, uint64_t ym, double* out2) {
+  cudaError_t e = launch_pauli(s->dt, s->amp, int(s->n), xm, zm, ym, s->scratch, s->d_small, s->stream, device_sms());
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(s->h_small, s->d_small, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return e;
+  out2[0] = s->h_small[0];
+  out2[1] = s->h_small[1];
+  return cudaSuccess;
+}
+
+cudaError_t state_inner(const StateImpl* a, const StateImpl* b, double* out2) {
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return e;
+  e = launch_inner(a->dt, a->amp, b->dt, b->amp, int(a->n), a->scratch, a->d_small, a->stream, device_sms());
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(a->h_small, a->d_small, 2 * sizeof(double), cudaMemcpyDeviceToHost, a->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(a->stream);
+  if (e != cudaSuccess) return e;
+  out2[0] = a->h_small[0];
+  out2[1] = a->h_small[1];
+  return cudaSuccess;
+}
+
+cudaError_t state_sample(const StateImpl* sc, const double* uniforms, uint32_t shots, uint64_t* out) {
+  StateImpl* s = const_cast<StateImpl*>(sc);
+  cudaError_t e;
+  if (s->shot_cap < shots) {
+    e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return e;
+    if (s->d_uni) cudaFree(s->d_uni);
+    if (s->d_shots) cudaFree(s->d_shots);
+    s->d_uni = nullptr;
+    s->d_shots = nullptr;
+    s->shot_cap = 0;
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&s->d_uni), sizeof(double) * shots)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&s->d_shots), sizeof(uint64_t) * shots)) != cudaSuccess) return e;
+    s->shot_cap = shots;
+  }
+  if ((e = cudaMemcpyAsync(s->d_uni, uniforms, sizeof(double) * shots, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) return e;
+  if ((e = launch_sample(s->dt, s->amp, int(s->n), s->d_uni, shots, s->scratch, s->d_shots, s->stream, device_sms())) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(out, s->d_shots, sizeof(uint64_t) * shots, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess) return e;
+  return cudaStreamSynchronize(s->stream);
+}
+
+// Probabilities in chunks through a device buffer (the full 2^n FP64 vector may
+// not fit next to the state).
+cudaError_t state_probabilities(const StateImpl* s, double* out) {
+  const uint64_t dim = 1ull << s->n;
+  const uint64_t chunk = std::min<uint64_t>(dim, 1ull << 24);
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d), chunk * sizeof(double));
+  if (e != cudaSuccess) return e;
+  const size_t ab = amp_bytes(s->dt);
+  for (uint64_t off = 0; off < dim && e == cudaSuccess; off += chunk) {
+    const uint64_t cnt = std::min(chunk, dim - off);
+    e = launch_probabilities(s->dt, static_cast<const char*>(s->amp) + off * ab, cnt, d, s->stream, device_sms());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out + off, d, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  }
+  cudaFree(d);
+  return e;
+}
+
+cudaError_t state_download_c128(const StateImpl* s, NqpuComplex* out) {
+  const uint64_t dim = 1ull << s->n;
+  if (s->dt == DType::C128) {
+    cudaError_t e = cudaMemcpyAsync(out, s->amp, dim * 16, cudaMemcpyDeviceToHost, s->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s->stream);
+  }
+  const uint64_t chunk = std::min<uint64_t>(dim, 1ull << 22);
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, chunk * 16);
+  if (e != cudaSuccess) return e;
+  for (uint64_t off = 0; off < dim && e == cudaSuccess; off += chunk) {
+    const uint64_t cnt = std::min(chunk, dim - off);
+    e = launch_convert(DType::C64, static_cast<const char*>(s->amp) + off * 8, DType::C128, d, cnt, s->stream, device_sms());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out + off, d, cnt * 16, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  }
+  cudaFree(d);
+  return e;
+}
+
+cudaError_t state_upload_c128(StateImpl* s, const NqpuComplex* in) {
+  const uint64_t dim = 1ull << s->n;
+  if (s->dt == DType::C128) {
+    cudaError_t e = cudaMemcpyAsync(s->amp, in, dim * 16, cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s->stream);
+  }
+  const uint64_t chunk = std::min<uint64_t>(dim, 1ull << 22);
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, chunk * 16);
+  if (e != cudaSuccess) return e;
+  for (uint64_t off = 0; off < dim && e == cudaSuccess; off += chunk) {
+    const uint64_t cnt = std::min(chunk, dim - off);
+    e = cudaMemcpyAsync(d, in + off, cnt * 16, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = launch_convert(DType::C128, d, DType::C64, static_cast<char*>(s->amp) + off * 8, cnt, s->stream, device_sms());
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  }
+  cudaFree(d);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Circuits
+// ---------------------------------------------------------------------------
+static void plan_free(DevicePlan* p) {
+  if (!p) return;
+  if (p->d_passes) cudaFree(p->d_passes);
+  if (p->d_stages) cudaFree(p->d_stages);
+  if (p->d_ops) cudaFree(p->d_ops);
+  if (p->fused) fused_plan_free(p->fused);
+  delete p;
+}
+
+void circuit_free(CircuitImpl* c) {
+  if (!c) return;
+  cudaDeviceSynchronize();
+  for (auto& kv : c->plans) plan_free(kv.second);
+  delete c;
+}
+
+static bool plan_host(const CircuitImpl* c, uint32_t n, DType dt, int mode, DevicePlan* p) {
+  p->ops = lower_circuit(c->gates);
+  p->stats = PlanStats{};
+  if (mode == NQPU_MODE_TILED && int(n) >= tile_min_qubits(dt)) {
+    std::string err;
+    if (!build_tile_plan(p->ops, int(n), dt, tile_kmax_for(dt), &p->tile, &err)) return false;
+    p->stats = p->tile.stats;
+  } else if (mode == NQPU_MODE_FUSED) {
+    p->stats.ops = p->ops.size();
+    return fused_plan_build(p->ops, int(n), dt, &p->fused, &p->stats);
+  } else {
+    p->stats.passes = p->ops.size();
+    p->stats.ops = p->ops.size();
+  }
+  return true;
+}
+
+bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out) {
+  DevicePlan p;
+  if (mode == NQPU_MODE_FUSED) {
+    p.ops = lower_circuit(c->gates);
+    bool ok = fused_plan_stats(p.ops, int(n), dt, out);
+    return ok;
+  }
+  if (!plan_host(c, n, dt, mode, &p)) return false;
+  *out = p.stats;
+  return true;
+}
+
+cudaError_t run_ops_pergate(StateImpl* s, const std::vector<Op>& ops) {
+  for (const Op& op : ops) {
+    cudaError_t e = launch_pergate(s->dt, s->amp, int(s->n), op, s->stream, device_sms());
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t upload_tile(DevicePlan* p) {
+  const TilePlan& t = p->tile;
+  cudaError_t e;
+  const size_t np = std::max<size_t>(1, t.passes.size());
+  const size_t ns = std::max<size_t>(1, t.stages.size());
+  const size_t opsz = t.dt == DType::C64 ? sizeof(TileOp<float>) : sizeof(TileOp<double>);
+  const size_t nops = t.dt == DType::C64 ? t.ops_f.size() : t.ops_d.size();
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&p->d_passes), np * sizeof(PassRec))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&p->d_stages), ns * sizeof(StageRec))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&p->d_ops, std::max<size_t>(1, nops) * opsz)) != cudaSuccess) return e;
+  if (!t.passes.empty() && (e = cudaMemcpy(p->d_passes, t.passes.data(), t.passes.size() * sizeof(PassRec), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+  if (!t.stages.empty() && (e = cudaMemcpy(p->d_stages, t.stages.data(), t.stages.size() * sizeof(StageRec), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+  if (nops) {
+    const void* src = t.dt == DType::C64 ? static_cast<const void*>(t.ops_f.data()) : static_cast<const void*>(t.ops_d.data());
+    if ((e = cudaMemcpy(p->d_ops, src, nops * opsz, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode) {
+  std::lock_guard<std::mutex> lk(c->mu);
+  const int effective = (mode == NQPU_MODE_TILED && int(s->n) < tile_min_qubits(s->dt)) ? int(NQPU_MODE_PERGATE) : mode;
+  const auto key = std::make_tuple(s->n, int(s->dt), effective);
+  DevicePlan*& p = c->plans[key];
+  if (p && p->version != c->version) {
+    cudaStreamSynchronize(s->stream);
+    plan_free(p);
+    p = nullptr;
+  }
+  if (!p) {
+    p = new DevicePlan();
+    if (!plan_host(c, s->n, s->dt, effective, p)) {
+      plan_free(p);
+      p = nullptr;
+      return cudaErrorInvalidValue;
+    }
+    if (effective == NQPU_MODE_TILED) {
+      cudaError_t e = upload_tile(p);
+      if (e != cudaSuccess) {
+        plan_free(p);
+        p = nullptr;
+        return e;
+      }
+    }
+    p->version = c->version;
+  }
+  if (effective == NQPU_MODE_PERGATE) return run_ops_pergate(s, p->ops);
+  if (effective == NQPU_MODE_FUSED) return fused_run(p->fused, s);
+  for (size_t i = 0; i < p->tile.passes.size(); ++i) {
+    cudaError_t e = launch_tile_pass(s->dt, s->amp, int(s->n), p->tile.passes[i], p->d_passes,
+                                     p->d_stages, p->d_ops, int(i), s->stream, device_sms());
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace nqpu

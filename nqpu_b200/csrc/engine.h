@@ -1,0 +1,75 @@
+// Engine objects behind the C ABI handles: device context, device-resident
+// states and circuits with their cached execution plans.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+#include "../../include/nqpu_b200.h"
+#include "planner.h"
+#include "sv_types.h"
+
+namespace nqpu {
+
+double next_random_f64();
+
+// Device context (one GPU; the engine uses the current device at first use).
+bool device_ready();
+int device_sms();
+
+struct StateImpl {
+  uint32_t n = 0;
+  DType dt = DType::C128;
+  void* amp = nullptr;         // 2^n amplitudes in HBM
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  double* scratch = nullptr;   // reduction scratch (reduce_scratch_bytes)
+  double* d_small = nullptr;   // small device outputs (256 doubles)
+  double* h_small = nullptr;   // pinned host mirror of d_small
+  double* d_uni = nullptr;     // sampling uniforms
+  uint64_t* d_shots = nullptr; // sampling outcomes
+  uint32_t shot_cap = 0;
+};
+
+StateImpl* state_new(uint32_t n, DType dt);
+void state_free(StateImpl* s);
+// out (n+1 values): [0] = sum|a|^2, [1+q] = sum over bit q set; either pointer may be null.
+cudaError_t state_zsums(const StateImpl* s, double* zs, double* total);
+cudaError_t state_pauli(const StateImpl* s, uint64_t xm, uint64_t zm, uint64_t ym, double* out2);
+cudaError_t state_inner(const StateImpl* a, const StateImpl* b, double* out2);
+cudaError_t state_sample(const StateImpl* s, const double* uniforms, uint32_t shots, uint64_t* out);
+cudaError_t state_probabilities(const StateImpl* s, double* out);
+cudaError_t state_download_c128(const StateImpl* s, NqpuComplex* out);
+cudaError_t state_upload_c128(StateImpl* s, const NqpuComplex* in);
+
+// Cached device plan of a circuit for one (state size, dtype, mode).
+struct DevicePlan {
+  uint64_t version = ~0ull;
+  TilePlan tile;
+  std::vector<Op> ops;         // lowered ops (per-gate mode)
+  PassRec* d_passes = nullptr;
+  StageRec* d_stages = nullptr;
+  void* d_ops = nullptr;
+  void* fused = nullptr;       // fused-mode plan (owned by the fused module)
+  PlanStats stats;
+};
+
+struct CircuitImpl {
+  uint32_t n = 0;
+  std::vector<GateRec> gates;
+  uint64_t version = 0;
+  std::map<std::tuple<uint32_t, int, int>, DevicePlan*> plans;
+  std::mutex mu;
+};
+
+void circuit_free(CircuitImpl* c);
+// Queue the circuit on the state's stream (no host sync).
+cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode);
+bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out);
+
+// Run a lowered op list on a state with the given mode (used by batch/server).
+cudaError_t run_ops_pergate(StateImpl* s, const std::vector<Op>& ops);
+
+}  // namespace nqpu

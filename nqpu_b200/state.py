@@ -1,0 +1,280 @@
+"""Python mirror of the reference's statevector interface over the C ABI.
+
+`StateVector` follows QuantumState + GateOperations (sdk/rust/src/lib.rs:326-1735)
+and the C FFI state/gate/measure calls (c_ffi.rs:789-1250); `Circuit` follows the
+C FFI circuit API (c_ffi.rs:1259-1400) extended to every GateType.  All work runs
+in the CUDA library; the Python layer only marshals arguments.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import NqpuComplex, NqpuMeasurement, check
+from .circuits import ARITY
+
+C128, C64 = 0, 1
+MODES = {"tiled": 0, "pergate": 1, "fused": 2}
+DTYPES = {"c128": C128, "complex128": C128, "c64": C64, "complex64": C64}
+
+
+def _cmat(m, size):
+    arr = np.asarray(m, dtype=np.complex128).reshape(-1)
+    if arr.size != size:
+        raise ValueError(f"matrix needs {size} entries")
+    buf = (NqpuComplex * size)()
+    for i, v in enumerate(arr):
+        buf[i].re = float(v.real)
+        buf[i].im = float(v.imag)
+    return buf
+
+
+_GATE_FN = {
+    "h": "nqpu_gate_h", "x": "nqpu_gate_x", "y": "nqpu_gate_y", "z": "nqpu_gate_z",
+    "s": "nqpu_gate_s", "t": "nqpu_gate_t", "sx": "nqpu_gate_sx", "rx": "nqpu_gate_rx",
+    "ry": "nqpu_gate_ry", "rz": "nqpu_gate_rz", "p": "nqpu_gate_phase", "u3": "nqpu_gate_u3",
+    "cx": "nqpu_gate_cx", "cz": "nqpu_gate_cz", "swap": "nqpu_gate_swap", "iswap": "nqpu_gate_iswap",
+    "cp": "nqpu_gate_cphase", "crx": "nqpu_gate_crx", "cry": "nqpu_gate_cry", "crz": "nqpu_gate_crz",
+    "rzz": "nqpu_gate_rzz", "rxx": "nqpu_gate_rxx", "ryy": "nqpu_gate_ryy", "ccx": "nqpu_gate_toffoli",
+    "ccz": "nqpu_gate_ccz", "cswap": "nqpu_gate_cswap", "cu": "nqpu_gate_cu",
+}
+_CIRC_FN = {
+    "h": "nqpu_circuit_add_h", "x": "nqpu_circuit_add_x", "y": "nqpu_circuit_add_y",
+    "z": "nqpu_circuit_add_z", "s": "nqpu_circuit_add_s", "t": "nqpu_circuit_add_t",
+    "sx": "nqpu_circuit_add_sx", "rx": "nqpu_circuit_add_rx", "ry": "nqpu_circuit_add_ry",
+    "rz": "nqpu_circuit_add_rz", "p": "nqpu_circuit_add_phase", "u3": "nqpu_circuit_add_u3",
+    "cx": "nqpu_circuit_add_cx", "cz": "nqpu_circuit_add_cz", "swap": "nqpu_circuit_add_swap",
+    "iswap": "nqpu_circuit_add_iswap", "cp": "nqpu_circuit_add_cphase", "crx": "nqpu_circuit_add_crx",
+    "cry": "nqpu_circuit_add_cry", "crz": "nqpu_circuit_add_crz", "rzz": "nqpu_circuit_add_rzz",
+    "rxx": "nqpu_circuit_add_rxx", "ryy": "nqpu_circuit_add_ryy", "ccx": "nqpu_circuit_add_toffoli",
+    "ccz": "nqpu_circuit_add_ccz", "cswap": "nqpu_circuit_add_cswap", "cu": "nqpu_circuit_add_cu",
+}
+
+
+class StateVector:
+    """Device-resident statevector (complex128 by default, like QuantumState)."""
+
+    def __init__(self, num_qubits: int, dtype: str = "c128"):
+        self.lib = _lib.load()
+        self.num_qubits = int(num_qubits)
+        self.dtype = DTYPES[dtype]
+        self.h_ = self.lib.nqpu_state_create_ex(self.num_qubits, self.dtype)
+        if not self.h_:
+            raise MemoryError(f"nqpu_state_create_ex({num_qubits}) failed (no CUDA device or out of memory)")
+
+    @classmethod
+    def _wrap(cls, lib, handle, n, dtype):
+        obj = cls.__new__(cls)
+        obj.lib, obj.h_, obj.num_qubits, obj.dtype = lib, handle, n, dtype
+        return obj
+
+    def close(self):
+        if getattr(self, "h_", None):
+            self.lib.nqpu_state_destroy(self.h_)
+            self.h_ = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def dim(self) -> int:
+        return 1 << self.num_qubits
+
+    # ---- state management ----
+    def clone(self) -> "StateVector":
+        h = self.lib.nqpu_state_clone(self.h_)
+        if not h:
+            raise MemoryError("nqpu_state_clone failed")
+        return StateVector._wrap(self.lib, h, self.num_qubits, self.dtype)
+
+    def reset(self):
+        check(self.lib.nqpu_state_reset(self.h_), "reset")
+
+    def set_basis(self, index: int):
+        check(self.lib.nqpu_state_set_basis(self.h_, int(index)), "set_basis")
+
+    def synchronize(self):
+        check(self.lib.nqpu_state_synchronize(self.h_), "synchronize")
+
+    def amplitude(self, index: int) -> complex:
+        out = NqpuComplex()
+        check(self.lib.nqpu_state_get_amplitude(self.h_, int(index), C.byref(out)), "get_amplitude")
+        return complex(out.re, out.im)
+
+    def set_amplitude(self, index: int, value: complex):
+        check(self.lib.nqpu_state_set_amplitude(self.h_, int(index), NqpuComplex(value.real, value.imag)),
+              "set_amplitude")
+
+    def amplitudes(self) -> np.ndarray:
+        out = np.empty(self.dim, dtype=np.complex128)
+        check(self.lib.nqpu_state_get_amplitudes(self.h_, out.ctypes.data_as(C.POINTER(NqpuComplex)), self.dim),
+              "get_amplitudes")
+        return out
+
+    def set_amplitudes(self, arr):
+        a = np.ascontiguousarray(np.asarray(arr, dtype=np.complex128).reshape(-1))
+        check(self.lib.nqpu_state_set_amplitudes(self.h_, a.ctypes.data_as(C.POINTER(NqpuComplex)), a.size),
+              "set_amplitudes")
+
+    def probabilities(self) -> np.ndarray:
+        out = np.empty(self.dim, dtype=np.float64)
+        check(self.lib.nqpu_state_probabilities(self.h_, out.ctypes.data_as(C.POINTER(C.c_double)), self.dim),
+              "probabilities")
+        return out
+
+    def norm(self) -> float:
+        return float(self.lib.nqpu_state_norm(self.h_))
+
+    def renormalize(self):
+        check(self.lib.nqpu_state_renormalize(self.h_), "renormalize")
+
+    # ---- gates (one kernel per gate) ----
+    def apply(self, name: str, qubits, params=(), matrix=None):
+        qs = [int(q) for q in qubits]
+        if name == "custom1":
+            return check(self.lib.nqpu_gate_custom_1q(self.h_, qs[0], _cmat(matrix, 4)), name)
+        if name == "custom2":
+            return check(self.lib.nqpu_gate_custom_2q(self.h_, qs[0], qs[1], _cmat(matrix, 16)), name)
+        if name == "u2lo":
+            return check(self.lib.nqpu_gate_u2(self.h_, qs[0], qs[1], _cmat(matrix, 16)), name)
+        fn = getattr(self.lib, _GATE_FN[name])
+        check(fn(self.h_, *qs, *[float(p) for p in params]), name)
+
+    def apply_gates(self, gates):
+        for g in gates:
+            self.apply(g[0], g[1], g[2] if len(g) > 2 else (), g[3] if len(g) > 3 else None)
+
+    def reset_qubit(self, q: int):
+        check(self.lib.nqpu_gate_reset_qubit(self.h_, int(q)), "reset_qubit")
+
+    # ---- reductions ----
+    def expectation_z(self, q: int) -> float:
+        out = C.c_double()
+        check(self.lib.nqpu_expectation_z(self.h_, int(q), C.byref(out)), "expectation_z")
+        return out.value
+
+    def expectation_z_all(self) -> np.ndarray:
+        out = np.empty(self.num_qubits, dtype=np.float64)
+        check(self.lib.nqpu_expectation_z_all(self.h_, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                              self.num_qubits), "expectation_z_all")
+        return out
+
+    def expectation_x(self, q: int) -> float:
+        out = C.c_double()
+        check(self.lib.nqpu_expectation_x(self.h_, int(q), C.byref(out)), "expectation_x")
+        return out.value
+
+    def expectation_y(self, q: int) -> float:
+        out = C.c_double()
+        check(self.lib.nqpu_expectation_y(self.h_, int(q), C.byref(out)), "expectation_y")
+        return out.value
+
+    def expectation_pauli_sum(self, terms) -> float:
+        """terms: list of (coeff, pauli_string of length n; char q acts on qubit q)."""
+        n = self.num_qubits
+        strs = b"".join(s.encode() for _, s in terms)
+        if any(len(s) != n for _, s in terms):
+            raise ValueError("each Pauli string needs one character per qubit")
+        coeffs = (C.c_double * max(1, len(terms)))(*[float(c) for c, _ in terms])
+        out = C.c_double()
+        check(self.lib.nqpu_expectation_pauli_sum(self.h_, strs, coeffs, len(terms), C.byref(out)),
+              "expectation_pauli_sum")
+        return out.value
+
+    def expectation_pauli_string(self, s: str) -> float:
+        return self.expectation_pauli_sum([(1.0, s)])
+
+    def fidelity(self, other: "StateVector") -> float:
+        out = C.c_double()
+        check(self.lib.nqpu_fidelity(self.h_, other.h_, C.byref(out)), "fidelity")
+        return out.value
+
+    def sample(self, shots: int) -> np.ndarray:
+        out = np.empty(shots, dtype=np.uint64)
+        check(self.lib.nqpu_sample(self.h_, int(shots), out.ctypes.data_as(C.POINTER(C.c_uint64))), "sample")
+        return out
+
+    def sample_with_uniforms(self, u) -> np.ndarray:
+        u = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
+        out = np.empty(u.size, dtype=np.uint64)
+        check(self.lib.nqpu_sample_with_uniforms(self.h_, u.ctypes.data_as(C.POINTER(C.c_double)), u.size,
+                                                 out.ctypes.data_as(C.POINTER(C.c_uint64))), "sample")
+        return out
+
+    def measure(self, q: int):
+        m = NqpuMeasurement()
+        check(self.lib.nqpu_measure(self.h_, int(q), C.byref(m)), "measure")
+        return int(m.outcome), float(m.probability)
+
+    def measure_all(self):
+        out = (C.c_uint32 * self.num_qubits)()
+        check(self.lib.nqpu_measure_all(self.h_, out, self.num_qubits), "measure_all")
+        return [int(v) for v in out]
+
+
+class Circuit:
+    """Circuit handle (nqpu_circuit_*); `execute` runs it on a StateVector."""
+
+    def __init__(self, num_qubits: int, gates=None, extended: bool = True):
+        self.lib = _lib.load()
+        self.num_qubits = int(num_qubits)
+        create = self.lib.nqpu_circuit_create_ex if extended else self.lib.nqpu_circuit_create
+        self.h_ = create(self.num_qubits)
+        if not self.h_:
+            raise ValueError(f"nqpu_circuit_create({num_qubits}) failed")
+        if gates:
+            self.extend(gates)
+
+    def close(self):
+        if getattr(self, "h_", None):
+            self.lib.nqpu_circuit_destroy(self.h_)
+            self.h_ = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, name: str, qubits, params=(), matrix=None):
+        qs = [int(q) for q in qubits]
+        if len(qs) != ARITY[name]:
+            raise ValueError(f"{name} takes {ARITY[name]} qubits")
+        if name == "custom1":
+            return check(self.lib.nqpu_circuit_add_custom_1q(self.h_, qs[0], _cmat(matrix, 4)), name)
+        if name == "custom2":
+            return check(self.lib.nqpu_circuit_add_custom_2q(self.h_, qs[0], qs[1], _cmat(matrix, 16)), name)
+        fn = getattr(self.lib, _CIRC_FN[name])
+        check(fn(self.h_, *qs, *[float(p) for p in params]), name)
+
+    def extend(self, gates):
+        for g in gates:
+            self.add(g[0], g[1], g[2] if len(g) > 2 else (), g[3] if len(g) > 3 else None)
+
+    def execute(self, state: StateVector, mode: str = "tiled"):
+        check(self.lib.nqpu_circuit_execute_ex(self.h_, state.h_, MODES[mode]), "circuit_execute")
+
+    @property
+    def gate_count(self) -> int:
+        return int(self.lib.nqpu_circuit_gate_count(self.h_))
+
+    @property
+    def depth(self) -> int:
+        return int(self.lib.nqpu_circuit_depth(self.h_))
+
+    def plan_stats(self, num_qubits: int, dtype: str = "c128", mode: str = "tiled"):
+        out = (C.c_uint64 * 3)()
+        check(self.lib.nqpu_circuit_plan_stats(self.h_, int(num_qubits), DTYPES[dtype], MODES[mode], out, 3),
+              "plan_stats")
+        return {"passes": int(out[0]), "ops": int(out[1]), "stages": int(out[2])}

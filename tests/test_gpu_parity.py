@@ -1,0 +1,392 @@
+"""GPU parity tests through the C ABI against the oracle.
+
+Tolerances (stated per precision):
+  complex128 engine vs FP64 oracle: max |amp diff| <= 1e-12, 1-F <= 1e-12,
+                                    max |d<Z_i>| <= 1e-12
+  complex64 engine vs FP64 oracle:  1-F <= 1e-5, max |d<Z_i>| <= 1e-5
+"""
+import math
+
+import numpy as np
+import pytest
+
+from nqpu_b200 import circuits
+from nqpu_b200.state import Circuit, StateVector
+from oracle.oracle import OracleState, xorshift_uniforms
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"c128": 1e-12, "c64": 1e-5}
+
+
+def fid(a, b):
+    return abs(np.vdot(a, b)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real)
+
+
+def random_unitary(rng, d):
+    q, r = np.linalg.qr(rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d)))
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def random_gate(rng, n, names=None):
+    names = names or [k for k in circuits.ARITY if circuits.ARITY[k] <= n]
+    name = names[int(rng.integers(len(names)))]
+    ar = circuits.ARITY[name]
+    qs = tuple(int(x) for x in rng.choice(n, size=ar, replace=False))
+    if name == "custom1":
+        return (name, qs, (), random_unitary(rng, 2))
+    if name in ("custom2", "u2lo"):
+        return (name, qs, (), random_unitary(rng, 4))
+    return (name, qs, tuple(float(x) for x in rng.uniform(-6, 6, size=4)))
+
+
+def random_circuit(rng, n, g, names=None):
+    # start from a random product state so every amplitude is non-trivial
+    gates = [("u3", (q,), tuple(float(x) for x in rng.uniform(0, 6, 3))) for q in range(n)]
+    return gates + [random_gate(rng, n, names) for _ in range(g)]
+
+
+def gate_names_for_circuit():
+    # the Circuit API has no u2lo entry (it is a GateOperations-only convention)
+    return [k for k in circuits.ARITY if k != "u2lo"]
+
+
+def check_close(gpu_amps, ref, dtype):
+    tol = TOL[dtype]
+    if dtype == "c128":
+        assert np.abs(gpu_amps - ref).max() <= 1e-12
+    assert 1 - fid(gpu_amps, ref) <= tol
+
+
+# ---------------------------------------------------------------------------
+# per-gate kernels
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+@pytest.mark.parametrize("n", [1, 2, 3, 6, 9])
+def test_pergate_every_gate(dtype, n):
+    rng = np.random.default_rng(100 + n)
+    names = [k for k in circuits.ARITY if circuits.ARITY[k] <= n]
+    for name in names:
+        for _ in range(3):
+            gates = [("u3", (q,), tuple(float(x) for x in rng.uniform(0, 6, 3))) for q in range(n)]
+            gates.append(random_gate(rng, n, [name]))
+            sv = StateVector(n, dtype)
+            sv.apply_gates(gates)
+            o = OracleState(n)
+            o.apply(gates)
+            check_close(sv.amplitudes(), o.amplitudes(), dtype)
+            sv.close()
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_pergate_exhaustive_placements(dtype):
+    n = 6
+    rng = np.random.default_rng(7)
+    prep = [("u3", (q,), tuple(float(x) for x in rng.uniform(0, 6, 3))) for q in range(n)]
+    o0 = OracleState(n)
+    o0.apply(prep)
+    base = o0.amplitudes()
+    sv = StateVector(n, dtype)
+    for a in range(n):
+        for b in range(n):
+            if a == b:
+                continue
+            for name in ("cx", "cz", "swap", "cp", "crx", "rzz", "custom2"):
+                g = random_gate(rng, n, [name])
+                g = (g[0], (a, b)) + tuple(g[2:])
+                sv.set_amplitudes(base)
+                sv.apply_gates([g])
+                o = OracleState(n)
+                o.set_amplitudes(base)
+                o.apply([g])
+                check_close(sv.amplitudes(), o.amplitudes(), dtype)
+
+
+# ---------------------------------------------------------------------------
+# tiled pass engine
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+@pytest.mark.parametrize("n", [4, 5, 6, 8, 11, 12, 13, 14, 16])
+def test_tiled_random_circuits(dtype, n):
+    rng = np.random.default_rng(1000 + n)
+    gates = random_circuit(rng, n, 12 * n, gate_names_for_circuit())
+    c = Circuit(n, gates)
+    sv = StateVector(n, dtype)
+    c.execute(sv, "tiled")
+    o = OracleState(n)
+    o.apply(gates)
+    check_close(sv.amplitudes(), o.amplitudes(), dtype)
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_brickwork_20q_config(dtype, seed):
+    # 20 qubits, |0..0>, 20 brickwork layers (U3 on every qubit + CNOT bricks)
+    n = 20
+    gates = circuits.brickwork(n, 20, seed)
+    c = Circuit(n, gates)
+    sv = StateVector(n, dtype)
+    c.execute(sv, "tiled")
+    o = OracleState(n)
+    o.apply(gates)
+    ref = o.amplitudes()
+    got = sv.amplitudes()
+    tol = TOL[dtype]
+    assert 1 - fid(got, ref) <= tol
+    z_ref = o.expectation_z_all()
+    z = sv.expectation_z_all()
+    assert np.abs(z - z_ref).max() <= tol
+    if dtype == "c128":
+        assert np.abs(got - ref).max() <= 1e-12
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_modes_agree(dtype):
+    n = 15
+    rng = np.random.default_rng(77)
+    gates = random_circuit(rng, n, 150, gate_names_for_circuit())
+    c = Circuit(n, gates)
+    a = StateVector(n, dtype)
+    b = StateVector(n, dtype)
+    c.execute(a, "tiled")
+    c.execute(b, "pergate")
+    assert 1 - a.fidelity(b) <= TOL[dtype]
+
+
+def test_circuit_reexecute_and_append():
+    n = 14
+    rng = np.random.default_rng(3)
+    gates = random_circuit(rng, n, 60, gate_names_for_circuit())
+    c = Circuit(n, gates[:40])
+    sv = StateVector(n, "c128")
+    c.execute(sv)
+    c.extend(gates[40:])  # plan cache must be rebuilt
+    sv.reset()
+    c.execute(sv)
+    o = OracleState(n)
+    o.apply(gates)
+    check_close(sv.amplitudes(), o.amplitudes(), "c128")
+
+
+# ---------------------------------------------------------------------------
+# reductions, sampling, measurement
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+@pytest.mark.parametrize("n", [1, 3, 7, 12, 13, 17])
+def test_reductions(dtype, n):
+    rng = np.random.default_rng(n)
+    gates = random_circuit(rng, n, 4 * n, gate_names_for_circuit())
+    sv = StateVector(n, dtype)
+    Circuit(n, gates).execute(sv)
+    o = OracleState(n)
+    o.apply(gates)
+    tol = 1e-12 if dtype == "c128" else 1e-5
+    np.testing.assert_allclose(sv.expectation_z_all(), o.expectation_z_all(), atol=tol, rtol=0)
+    for q in range(n):
+        assert abs(sv.expectation_z(q) - o.expectation_z_all()[q]) <= tol
+        assert abs(sv.expectation_x(q) - o.expectation_x(q)) <= tol
+        assert abs(sv.expectation_y(q) - o.expectation_y(q)) <= tol
+    assert abs(sv.norm() - o.norm()) <= tol
+    np.testing.assert_allclose(sv.probabilities(), o.probabilities(), atol=tol, rtol=0)
+    terms = []
+    for _ in range(6):
+        s = "".join("IXYZ"[int(x)] for x in rng.integers(0, 4, size=n))
+        terms.append((float(rng.uniform(-1, 1)), s))
+    ref = sum(cf * o.pauli_string(s) for cf, s in terms)
+    assert abs(sv.expectation_pauli_sum(terms) - ref) <= 10 * tol
+
+
+def test_fidelity_across_dtypes():
+    n = 16
+    gates = circuits.brickwork(n, 10, 5)
+    a = StateVector(n, "c128")
+    b = StateVector(n, "c64")
+    c = Circuit(n, gates)
+    c.execute(a)
+    c.execute(b)
+    o = OracleState(n)
+    o.apply(gates)
+    o32 = OracleState(n, f32=True)
+    o32.apply(gates)
+    f = a.fidelity(b)
+    assert abs(f - o.fidelity(o32)) < 1e-5
+    assert 1 - f <= 1e-5
+    assert abs(a.fidelity(a) - 1) < 1e-12
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+@pytest.mark.parametrize("n", [2, 10, 14])
+def test_sampling_matches_oracle_rule(dtype, n):
+    gates = circuits.brickwork(n, 6, 11)
+    sv = StateVector(n, dtype)
+    Circuit(n, gates).execute(sv)
+    o = OracleState(n)
+    o.apply(gates)
+    u = xorshift_uniforms(1234, 4000)
+    got = sv.sample_with_uniforms(u)
+    ref = o.sample_uniforms(u)
+    mismatch = np.count_nonzero(got != ref)
+    if dtype == "c128":
+        assert mismatch <= 2  # only CDF summation-order ties at segment boundaries
+    else:
+        assert mismatch <= 40  # complex64 CDF rounding moves rare boundary draws
+    # statistical check against exact probabilities (total variation distance)
+    p = o.probabilities()
+    hist = np.bincount(got.astype(np.int64), minlength=1 << n) / len(got)
+    assert 0.5 * np.abs(hist - p).sum() < (0.08 if n <= 10 else 0.5)
+
+
+def test_seeded_sample_is_reference_stream(lib):
+    n = 8
+    gates = circuits.brickwork(n, 5, 2)
+    sv = StateVector(n, "c128")
+    Circuit(n, gates).execute(sv)
+    lib.nqpu_set_seed(99)
+    s1 = sv.sample(1000)
+    lib.nqpu_set_seed(99)
+    s2 = sv.sample(1000)
+    assert np.array_equal(s1, s2)  # c_ffi.rs:2478 seed determinism
+    o = OracleState(n)
+    o.apply(gates)
+    ref = o.sample_uniforms(xorshift_uniforms(99, 1000))
+    assert np.count_nonzero(s1 != ref) <= 2
+
+
+def test_bell_sampling_and_measure(lib):
+    sv = StateVector(2)
+    sv.apply_gates([("h", (0,), ()), ("cx", (0, 1), ())])
+    lib.nqpu_set_seed(5)
+    s = sv.sample(1000)
+    assert set(np.unique(s)) <= {0, 3}
+    assert 0 < np.count_nonzero(s == 0) < 1000  # c_ffi.rs:2240
+    # measure |0> always 0, |1> always 1 (c_ffi.rs:1852, :1871)
+    z = StateVector(3)
+    for _ in range(10):
+        assert z.measure(1) == (0, pytest.approx(1.0))
+    one = StateVector(3)
+    one.apply_gates([("x", (2,), ())])
+    for _ in range(10):
+        assert one.measure(2) == (1, pytest.approx(1.0))
+    # collapse: measuring a Bell pair leaves |00> or |11>
+    lib.nqpu_set_seed(17)
+    out, p = sv.measure(0)
+    assert abs(p - 0.5) < 1e-12
+    a = sv.amplitudes()
+    assert abs(abs(a[3 * out]) - 1) < 1e-12
+    # seeded measurement follows the reference rule: r < prob0 -> 0
+    r = xorshift_uniforms(17, 1)[0]
+    assert out == (0 if r < 0.5 else 1)
+
+
+def test_measure_all_and_reset_qubit():
+    sv = StateVector(4)
+    sv.apply_gates([("x", (1,), ()), ("x", (3,), ())])
+    assert sv.measure_all() == [0, 1, 0, 1]
+    n = 6
+    gates = circuits.brickwork(n, 4, 8)
+    sv = StateVector(n)
+    sv.apply_gates(gates)
+    sv.reset_qubit(2)
+    o = OracleState(n)
+    o.apply(gates)
+    o.reset_qubit(2)
+    check_close(sv.amplitudes(), o.amplitudes(), "c128")
+
+
+# ---------------------------------------------------------------------------
+# reference known-answer tests through the C ABI (c_ffi.rs:1646-2660)
+# ---------------------------------------------------------------------------
+def test_c_ffi_known_answers(lib):
+    import ctypes as C
+    from nqpu_b200._lib import NqpuComplex
+    EPS = 1e-10
+    s2 = 1 / math.sqrt(2)
+    st = lib.nqpu_state_create(5)
+    assert st and lib.nqpu_state_num_qubits(st) == 5
+    a = NqpuComplex()
+    assert lib.nqpu_state_get_amplitude(st, 0, C.byref(a)) == 0 and abs(a.re - 1) < EPS
+    for i in range(1, 32):
+        lib.nqpu_state_get_amplitude(st, i, C.byref(a))
+        assert abs(a.re) < EPS and abs(a.im) < EPS
+    assert lib.nqpu_state_get_amplitude(st, 32, C.byref(a)) == 2
+    assert lib.nqpu_state_set_amplitude(st, 3, NqpuComplex(0.6, 0.8)) == 0
+    lib.nqpu_state_get_amplitude(st, 3, C.byref(a))
+    assert abs(a.re - 0.6) < EPS and abs(a.im - 0.8) < EPS
+    assert lib.nqpu_state_reset(st) == 0
+    lib.nqpu_state_get_amplitude(st, 0, C.byref(a))
+    assert abs(a.re - 1) < EPS
+    # invalid qubits / same-qubit errors
+    assert lib.nqpu_gate_h(st, 5) == 1
+    assert lib.nqpu_gate_cx(st, 0, 5) == 1
+    assert lib.nqpu_gate_cx(st, 0, 0) == 2
+    assert lib.nqpu_gate_cz(st, 1, 1) == 2
+    assert lib.nqpu_gate_swap(st, 0, 0) == 2
+    assert lib.nqpu_gate_rx(st, 0, float("nan")) == 2
+    lib.nqpu_state_destroy(st)
+
+    st = lib.nqpu_state_create(2)
+    assert lib.nqpu_gate_h(st, 0) == 0 and lib.nqpu_gate_cx(st, 0, 1) == 0
+    amps = []
+    for i in range(4):
+        lib.nqpu_state_get_amplitude(st, i, C.byref(a))
+        amps.append(complex(a.re, a.im))
+    assert abs(amps[0] - s2) < EPS and abs(amps[3] - s2) < EPS
+    d = C.c_double()
+    lib.nqpu_expectation_z(st, 0, C.byref(d))
+    assert abs(d.value) < EPS
+    assert abs(lib.nqpu_state_norm(st) - 1) < EPS
+    probs = (C.c_double * 4)()
+    assert lib.nqpu_state_probabilities(st, probs, 4) == 0
+    assert abs(sum(probs) - 1) < EPS
+    assert lib.nqpu_state_probabilities(st, probs, 3) == 2
+    # clone independence (c_ffi.rs:1937)
+    cl = lib.nqpu_state_clone(st)
+    lib.nqpu_gate_x(cl, 0)
+    lib.nqpu_state_get_amplitude(st, 0, C.byref(a))
+    assert abs(a.re - s2) < EPS
+    lib.nqpu_state_get_amplitude(cl, 0, C.byref(a))
+    assert abs(a.re) < EPS
+    lib.nqpu_state_destroy(cl)
+    lib.nqpu_state_destroy(st)
+
+    # custom 1q identity, custom 2q SWAP (q1 high) (c_ffi.rs:2135, :2168)
+    st = lib.nqpu_state_create(2)
+    lib.nqpu_gate_h(st, 0)
+    ident = (NqpuComplex * 4)(NqpuComplex(1, 0), NqpuComplex(0, 0), NqpuComplex(0, 0), NqpuComplex(1, 0))
+    assert lib.nqpu_gate_custom_1q(st, 0, ident) == 0
+    lib.nqpu_state_get_amplitude(st, 1, C.byref(a))
+    assert abs(a.re - s2) < EPS
+    lib.nqpu_state_destroy(st)
+    st = lib.nqpu_state_create(2)
+    lib.nqpu_gate_x(st, 1)  # |10> index 2
+    sw = (NqpuComplex * 16)()
+    for i, j in ((0, 0), (1, 2), (2, 1), (3, 3)):
+        sw[i * 4 + j] = NqpuComplex(1, 0)
+    assert lib.nqpu_gate_custom_2q(st, 1, 0, sw) == 0
+    lib.nqpu_state_get_amplitude(st, 1, C.byref(a))
+    assert abs(a.re - 1) < EPS
+    lib.nqpu_state_destroy(st)
+
+    # circuit execute (c_ffi.rs:2007)
+    c = lib.nqpu_circuit_create(2)
+    lib.nqpu_circuit_add_h(c, 0)
+    lib.nqpu_circuit_add_cx(c, 0, 1)
+    st = lib.nqpu_state_create(2)
+    assert lib.nqpu_circuit_execute(c, st) == 0
+    lib.nqpu_state_get_amplitude(st, 3, C.byref(a))
+    assert abs(a.re - s2) < EPS
+    big = lib.nqpu_circuit_create(3)
+    assert lib.nqpu_circuit_execute(big, st) == 2  # circuit wider than state
+    lib.nqpu_circuit_destroy(big)
+    lib.nqpu_circuit_destroy(c)
+    lib.nqpu_state_destroy(st)
+
+
+def test_norm_preserved_many_gates():
+    n = 12
+    rng = np.random.default_rng(21)
+    gates = random_circuit(rng, n, 500, [k for k in gate_names_for_circuit() if not k.startswith("custom")])
+    for dtype in ("c128", "c64"):
+        sv = StateVector(n, dtype)
+        Circuit(n, gates).execute(sv)
+        assert abs(sv.norm() - 1) < (1e-12 if dtype == "c128" else 1e-5)
