@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the statevector circuit-run path on B200.
+
+Default workload (one step = one full circuit run):
+  30-qubit random brickwork circuit, depth 40 (1200 U3 + 580 CNOT = 1780 gates),
+  complex64 state (8 GiB, larger than L2 -> no flush needed), |0..0> reset,
+  every gate applied unfused by the tiled pass engine, then all <Z_i> (FP64).
+  metric = gates/s (original gates per second, whole job over all ranks).
+
+Also reported (one untimed run each): the complex128 run of the same circuit
+and 1-F / max|d<Z_i>| of complex64 against it; the plain per-gate path (one
+kernel launch per gate) and its algorithmic HBM GB/s.
+
+  python bench.py [--gpus N --steps K --warmup W]     engine arm
+  python bench.py --impl reference                   CPU reference arm (oracle port)
+
+Multi-GPU: the path does not shard (one state per GPU), so N ranks run N
+independent replicas ("weak" scaling); value = all ranks' gates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            if self.uuid and self.uuid not in parts[0]:
+                continue
+            rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_rate(gates, n, f32, budget_s, threads=0):
+    """Oracle (CPU restatement of the reference path) gates/s on a bounded
+    prefix of the circuit: gates are applied one by one until `budget_s`."""
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    st = O.OracleState(n, f32=f32)
+    done, t0 = 0, time.perf_counter()
+    while done < len(gates) and time.perf_counter() - t0 < budget_s:
+        st.apply([gates[done]])
+        done += 1
+    el = time.perf_counter() - t0
+    return done / el, done, el, O.max_threads()
+
+
+def run_reference(args):
+    from nqpu_b200.circuits import brickwork
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n, depth = args.qubits, args.depth
+    gates = brickwork(n, depth, args.seed)
+    f32 = args.dtype == "c64"
+    # warm-up: untimed gate applications (page the 8-16 GiB host state in)
+    from oracle import oracle as O
+    st = O.OracleState(n, f32=f32)
+    for i in range(args.warmup):
+        st.apply([gates[i % len(gates)]])
+    # each step applies a bounded slice of the circuit (~`--ref-step-s` seconds)
+    t0 = time.perf_counter()
+    st.apply([gates[0]])
+    per_gate = time.perf_counter() - t0
+    g_step = max(1, int(args.ref_step_s / max(per_gate, 1e-6)))
+    times, cnt, pos = [], 0, 1
+    for _ in range(args.steps):
+        sl = [gates[(pos + j) % len(gates)] for j in range(g_step)]
+        t0 = time.perf_counter()
+        st.apply(sl)
+        times.append(time.perf_counter() - t0)
+        cnt += g_step
+        pos += g_step
+    el = sum(times)
+    value = cnt / el
+    cores = O.max_threads()
+    line = {
+        "impl": "reference", "metric": "gates/s (30q complex64 brickwork, unfused)", "value": value,
+        "unit": "gates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64" if f32 else "c128", "data": "synthetic",
+        "config": {"workload": f"brickwork {n}q depth {depth} {'complex64' if f32 else 'complex128'}",
+                   "gates": len(gates), "seed": args.seed},
+        "cpu_baseline": {"value": value, "unit": "gates/s", "cores": cores, "kind": "port",
+                         "sample": f"{g_step} gates per step x {args.steps} steps of the {n}q circuit, "
+                                   f"per-gate full passes, OpenMP {cores} threads"},
+        "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def traffic_from_profile(n, amp_bytes):
+    """DRAM traffic per tiled-pass launch from the committed ncu summary
+    (bytes per amplitude per pass, scaled to this state size)."""
+    p = ROOT / "profiles" / "tile_pass_c64.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_amplitude_per_pass:"):
+            try:
+                return float(line.split(":")[1].split()[0]) * (1 << n)
+            except ValueError:
+                return None
+    return None
+
+
+def run_engine(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+
+    from nqpu_b200 import _lib
+    from nqpu_b200.circuits import brickwork
+    from nqpu_b200.state import Circuit, StateVector, MODES
+    lib = _lib.load()
+
+    n, depth = args.qubits, args.depth
+    gates = brickwork(n, depth, args.seed)
+    G = len(gates)
+    amp_bytes = 8 if args.dtype == "c64" else 16
+    S = (1 << n) * amp_bytes
+    circ = Circuit(n, gates)
+    stats = circ.plan_stats(n, args.dtype, args.mode)
+    sv = StateVector(n, args.dtype)
+    stream = torch.cuda.ExternalStream(lib.nqpu_state_cuda_stream(sv.h_), device=dev)
+    zout = np.empty(n, dtype=np.float64)
+    zptr = zout.ctypes.data_as(C.POINTER(C.c_double))
+    maxl = 4096
+    lms = (C.c_float * maxl)()
+    cnt = C.c_uint32()
+
+    def step(profile=False):
+        _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
+        if profile:
+            _lib.check(lib.nqpu_circuit_profile(circ.h_, sv.h_, MODES[args.mode], lms, maxl, C.byref(cnt)), "profile")
+        else:
+            _lib.check(lib.nqpu_circuit_execute_ex(circ.h_, sv.h_, MODES[args.mode]), "execute")
+        _lib.check(lib.nqpu_expectation_z_all(sv.h_, zptr, n), "zall")
+
+    for _ in range(args.warmup):
+        step()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sv.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    launch_ms = []
+    for _ in range(args.steps):
+        step(profile=True)
+        launch_ms.extend(lms[i] for i in range(cnt.value))
+    ev1.record(stream)
+    ev1.synchronize()
+    sv.synchronize()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    el_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([el_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el_ms = float(t.item())
+    total_gates = G * args.steps * world
+    value = total_gates / (el_ms / 1000.0)
+    z_c64 = zout.copy()
+
+    # roofline of the dominant kernel (the tiled pass): 2S algorithmic bytes per launch
+    peak, peak_kind = peaks()
+    avg_launch_ms = float(np.mean(launch_ms)) if launch_ms else float("nan")
+    achieved = 2 * S / (avg_launch_ms / 1000.0) / 1e9
+    traffic = traffic_from_profile(n, amp_bytes)
+    roofline = {"bound": "hbm", "kernel": "k_tile_pass", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
+                "launches_per_step": stats["passes"], "avg_launch_ms": avg_launch_ms,
+                "pass_time_share": (sum(launch_ms) / el_ms) if el_ms else None}
+    launches_per_step = stats["passes"] + 1 + 2  # passes + reset + zsums (2 kernels)
+
+    extra = {}
+    if rank == 0 and world == 1 and not args.quick:
+        # accuracy: complex64 against the complex128 (FP64) run of the same circuit
+        ref_dtype = "c128" if args.dtype == "c64" else None
+        if ref_dtype:
+            sv128 = StateVector(n, ref_dtype)
+            t0 = time.perf_counter()
+            circ.execute(sv128, args.mode)
+            z128 = sv128.expectation_z_all()
+            t128 = time.perf_counter() - t0
+            f = sv.fidelity(sv128)
+            extra["accuracy_vs_fp64"] = {"one_minus_F": 1.0 - f, "max_abs_dZ": float(np.abs(z_c64 - z128).max()),
+                                         "tolerance": {"one_minus_F": 1e-5, "max_abs_dZ": 1e-5}}
+            extra["complex128_run"] = {"gates_per_s": G / t128, "seconds": t128,
+                                       "passes": circ.plan_stats(n, "c128", args.mode)["passes"]}
+            sv128.close()
+        # plain per-gate path: one launch per gate, algorithmic GB/s
+        pg_ms = (C.c_float * maxl)()
+        pcnt = C.c_uint32()
+        _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
+        lib.nqpu_circuit_execute_ex(circ.h_, sv.h_, MODES["pergate"])  # warm
+        _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
+        _lib.check(lib.nqpu_circuit_profile(circ.h_, sv.h_, MODES["pergate"], pg_ms, maxl, C.byref(pcnt)), "profile")
+        from nqpu_b200.circuits import algorithmic_bytes
+        tot_ms = sum(pg_ms[i] for i in range(pcnt.value))
+        u3_ms = [pg_ms[i] for i in range(pcnt.value) if gates[i][0] == "u3"]
+        cx_ms = [pg_ms[i] for i in range(pcnt.value) if gates[i][0] == "cx"]
+        extra["pergate_path"] = {
+            "gates_per_s": G / (tot_ms / 1000), "seconds": tot_ms / 1000,
+            "algorithmic_GBps": algorithmic_bytes(gates, n, amp_bytes) / (tot_ms / 1000) / 1e9,
+            "u3_GBps": 2 * S / (np.mean(u3_ms) / 1000) / 1e9 if u3_ms else None,
+            "cnot_GBps": S / (np.mean(cx_ms) / 1000) / 1e9 if cx_ms else None,
+            "frac_of_peak": algorithmic_bytes(gates, n, amp_bytes) / (tot_ms / 1000) / 1e9 / peak,
+        }
+
+    # e2e: host gate list -> circuit handle -> execute (plan build + H2D) -> <Z_i> D2H
+    e2e = None
+    if not args.quick:
+        torch.cuda.synchronize(dev)
+        h2d = stats.get("upload_bytes", 0)
+        t_e2e = []
+        for _ in range(max(1, args.e2e_steps)):
+            t0 = time.perf_counter()
+            c2 = Circuit(n, gates)
+            _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
+            _lib.check(lib.nqpu_circuit_execute_ex(c2.h_, sv.h_, MODES[args.mode]), "execute")
+            _lib.check(lib.nqpu_expectation_z_all(sv.h_, zptr, n), "zall")
+            t_e2e.append(time.perf_counter() - t0)
+            c2.close()
+        et = float(np.mean(t_e2e))
+        if world > 1:
+            t = torch.tensor([et], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        e2e = {"value": G * world / et, "unit": "gates/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": 8 * n, "seconds_per_step": et,
+               "timing": "host wall clock around create+execute+reduce (includes plan build)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.quick and not args.no_cpu:
+        rate, done, el, cores = cpu_reference_rate(gates, n, args.dtype == "c64", args.cpu_budget_s)
+        cpu = {"value": rate, "unit": "gates/s", "cores": cores, "kind": "port",
+               "sample": f"first {done} gates of the {n}q circuit in {el:.1f} s, per-gate full passes"}
+
+    if rank == 0:
+        line = {
+            "metric": "gates/s (30q complex64 brickwork, unfused)", "value": value, "unit": "gates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": f"brickwork {n}q depth {depth} {'complex64' if args.dtype == 'c64' else 'complex128'}",
+                       "gates": G, "seed": args.seed, "engine_mode": args.mode,
+                       "plan": {"passes": stats["passes"], "stages": stats["stages"]},
+                       "l2": "state 8 GiB >> 126 MB L2; no flush", "parallelism": f"replicas{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps, "clocks": clk,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    sv.close()
+    circ.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=40)
+    ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
+    ap.add_argument("--mode", default="tiled", choices=["tiled", "pergate", "fused"])
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget-s", type=float, default=15.0)
+    ap.add_argument("--ref-step-s", type=float, default=4.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="timed region only (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3 and not args.quick:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -161,6 +161,8 @@ NqpuError   nqpu_state_get_amplitudes(const NqpuState* state, NqpuComplex* out, 
 NqpuError   nqpu_state_set_amplitudes(NqpuState* state, const NqpuComplex* in, uint64_t len);
 /* Block until all work queued on the state's stream has finished. */
 NqpuError   nqpu_state_synchronize(const NqpuState* state);
+/* The cudaStream_t the state's work is queued on (for CUDA-event timing). */
+void*       nqpu_state_cuda_stream(const NqpuState* state);
 
 /* Reference GateOperations coverage (R/lib.rs:617-1735, gates.rs). */
 NqpuError   nqpu_gate_sx(NqpuState* state, uint32_t qubit);
@@ -236,9 +238,14 @@ NqpuError    nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uint32_t q2
 NqpuCircuit* nqpu_circuit_create_ex(uint32_t num_qubits);
 /* Run with an explicit engine mode. */
 NqpuError    nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode);
+/* Run the circuit recording a CUDA event between consecutive kernel launches;
+ * launch_ms[i] = device time of launch i (i < *count <= len). */
+NqpuError    nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,
+                                  float* launch_ms, uint32_t len, uint32_t* count);
 /* Plan statistics of the last execution of `circuit` in `mode` on an n-qubit state:
  * out[0] = HBM passes (kernel launches over the full state), out[1] = lowered ops,
- * out[2] = register stages (tiled) or fused unitaries (fused).  len >= 3. */
+ * out[2] = register stages (tiled) or fused unitaries (fused), out[3] (when
+ * len >= 4) = bytes of plan tables uploaded host->device per plan build.  len >= 3. */
 NqpuError    nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_t num_qubits,
                                      NqpuDtype dtype, NqpuMode mode, uint64_t* out, uint32_t len);
 

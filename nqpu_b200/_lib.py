@@ -35,6 +35,7 @@ _SCALARS = {
     "uint64_t": C.c_uint64,
     "int": C.c_int,
     "double": C.c_double,
+    "float": C.c_float,
     "NqpuError": C.c_int,
     "NqpuDtype": C.c_int,
     "NqpuMode": C.c_int,

@@ -32,6 +32,10 @@ ARITY = {name: (3 if name in ("ccx", "ccz", "cswap") else
                               "ryy", "custom2", "u2lo", "cu") else 1)
          for name in GATE_CODES}
 
+NPARAMS = {name: 0 for name in GATE_CODES}
+NPARAMS.update({"rx": 1, "ry": 1, "rz": 1, "p": 1, "u3": 3, "cp": 1, "crx": 1, "cry": 1, "crz": 1,
+                "rzz": 1, "rxx": 1, "ryy": 1, "cu": 4})
+
 FLAT_WIDTH = 40  # code, q0, q1, q2, p0..p3, 16 complex matrix entries (re, im)
 
 
@@ -42,6 +46,7 @@ def flatten(gates) -> np.ndarray:
         name, qs, ps = g[0], g[1], g[2]
         out[i, 0] = GATE_CODES[name]
         out[i, 1:1 + len(qs)] = qs
+        ps = tuple(ps)[:NPARAMS[name]]
         out[i, 4:4 + len(ps)] = ps
         if len(g) > 3 and g[3] is not None:
             m = np.asarray(g[3], dtype=np.complex128).reshape(-1)

@@ -112,6 +112,10 @@ extern "C" NqpuDtype nqpu_state_dtype(const NqpuState* state) {
   return (state && S(state)->dt == DType::C64) ? NQPU_C64 : NQPU_C128;
 }
 
+extern "C" void* nqpu_state_cuda_stream(const NqpuState* state) {
+  return state ? static_cast<void*>(S(state)->stream) : nullptr;
+}
+
 extern "C" NqpuError nqpu_state_synchronize(const NqpuState* state) {
   if (!state) return NQPU_NULL_POINTER;
   NQ_TRY(cudaStreamSynchronize(S(state)->stream));
@@ -602,6 +606,28 @@ extern "C" NqpuError nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuSta
   return NQPU_OK;
 }
 
+extern "C" NqpuError nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,
+                                          float* launch_ms, uint32_t len, uint32_t* count) {
+  if (!circuit || !state || !launch_ms || !count) return NQPU_NULL_POINTER;
+  const CircuitImpl* c = Cc(circuit);
+  StateImpl* s = S(state);
+  if (c->n > s->n) return NQPU_INVALID_PARAMETER;
+  std::vector<cudaEvent_t> ev;
+  cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode), &ev);
+  cudaError_t e2 = cudaStreamSynchronize(s->stream);
+  uint32_t k = 0;
+  for (size_t i = 0; i + 1 < ev.size() && k < len; ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+    launch_ms[k++] = ms;
+  }
+  for (auto x : ev) cudaEventDestroy(x);
+  *count = k;
+  if (e != cudaSuccess) return map_cuda(e);
+  if (e2 != cudaSuccess) return map_cuda(e2);
+  return NQPU_OK;
+}
+
 extern "C" NqpuError nqpu_circuit_execute(const NqpuCircuit* circuit, NqpuState* state) {
   return nqpu_circuit_execute_ex(circuit, state, NQPU_MODE_TILED);
 }
@@ -626,6 +652,7 @@ extern "C" NqpuError nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_
   out[0] = st.passes;
   out[1] = st.ops;
   out[2] = st.stages;
+  if (len >= 4) out[3] = st.upload_bytes;
   return NQPU_OK;
 }
 

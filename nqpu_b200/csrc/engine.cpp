@@ -275,7 +275,16 @@ static cudaError_t upload_tile(DevicePlan* p) {
   return cudaSuccess;
 }
 
-cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode) {
+static cudaError_t mark(std::vector<cudaEvent_t>* ev, cudaStream_t st) {
+  if (!ev) return cudaSuccess;
+  cudaEvent_t e;
+  cudaError_t r = cudaEventCreate(&e);
+  if (r != cudaSuccess) return r;
+  ev->push_back(e);
+  return cudaEventRecord(e, st);
+}
+
+cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cudaEvent_t>* events) {
   std::lock_guard<std::mutex> lk(c->mu);
   const int effective = (mode == NQPU_MODE_TILED && int(s->n) < tile_min_qubits(s->dt)) ? int(NQPU_MODE_PERGATE) : mode;
   const auto key = std::make_tuple(s->n, int(s->dt), effective);
@@ -302,12 +311,21 @@ cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode) {
     }
     p->version = c->version;
   }
-  if (effective == NQPU_MODE_PERGATE) return run_ops_pergate(s, p->ops);
-  if (effective == NQPU_MODE_FUSED) return fused_run(p->fused, s);
+  cudaError_t e = mark(events, s->stream);
+  if (e != cudaSuccess) return e;
+  if (effective == NQPU_MODE_PERGATE) {
+    for (const Op& op : p->ops) {
+      if ((e = launch_pergate(s->dt, s->amp, int(s->n), op, s->stream, device_sms())) != cudaSuccess) return e;
+      if ((e = mark(events, s->stream)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  if (effective == NQPU_MODE_FUSED) return fused_run(p->fused, s, events);
   for (size_t i = 0; i < p->tile.passes.size(); ++i) {
-    cudaError_t e = launch_tile_pass(s->dt, s->amp, int(s->n), p->tile.passes[i], p->d_passes,
-                                     p->d_stages, p->d_ops, int(i), s->stream, device_sms());
+    e = launch_tile_pass(s->dt, s->amp, int(s->n), p->tile.passes[i], p->d_passes, p->d_stages,
+                         p->d_ops, int(i), s->stream, device_sms());
     if (e != cudaSuccess) return e;
+    if ((e = mark(events, s->stream)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

@@ -65,8 +65,10 @@ struct CircuitImpl {
 };
 
 void circuit_free(CircuitImpl* c);
-// Queue the circuit on the state's stream (no host sync).
-cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode);
+// Queue the circuit on the state's stream (no host sync).  With `events`, an
+// event is recorded before the first launch and after every launch.
+cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode,
+                        std::vector<cudaEvent_t>* events = nullptr);
 bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out);
 
 // Run a lowered op list on a state with the given mode (used by batch/server).

@@ -10,5 +10,5 @@ struct StateImpl;
 bool fused_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, PlanStats* stats);
 bool fused_plan_stats(const std::vector<Op>& ops, int n, DType dt, PlanStats* stats);
 void fused_plan_free(void* plan);
-cudaError_t fused_run(void* plan, StateImpl* s);
+cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events);
 }  // namespace nqpu

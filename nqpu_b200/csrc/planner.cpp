@@ -418,6 +418,8 @@ bool build_tile_plan(const std::vector<Op>& ops, int n, DType dt, int kmax, Tile
   out->stats.passes = out->passes.size();
   out->stats.ops = ops.size();
   out->stats.stages = out->stages.size();
+  out->stats.upload_bytes = out->passes.size() * sizeof(PassRec) + out->stages.size() * sizeof(StageRec) +
+                            out->ops_f.size() * sizeof(TileOp<float>) + out->ops_d.size() * sizeof(TileOp<double>);
   return true;
 }
 

@@ -121,7 +121,7 @@ struct TileOp {
 };
 
 struct PlanStats {
-  uint64_t passes = 0, ops = 0, stages = 0;
+  uint64_t passes = 0, ops = 0, stages = 0, upload_bytes = 0;
 };
 
 }  // namespace nqpu

@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import NqpuComplex, NqpuMeasurement, check
-from .circuits import ARITY
+from .circuits import ARITY, NPARAMS
 
 C128, C64 = 0, 1
 MODES = {"tiled": 0, "pergate": 1, "fused": 2}
@@ -149,7 +149,10 @@ class StateVector:
         if name == "u2lo":
             return check(self.lib.nqpu_gate_u2(self.h_, qs[0], qs[1], _cmat(matrix, 16)), name)
         fn = getattr(self.lib, _GATE_FN[name])
-        check(fn(self.h_, *qs, *[float(p) for p in params]), name)
+        ps = [float(p) for p in tuple(params)[:NPARAMS[name]]]
+        if len(ps) != NPARAMS[name]:
+            raise ValueError(f"{name} takes {NPARAMS[name]} parameters")
+        check(fn(self.h_, *qs, *ps), name)
 
     def apply_gates(self, gates):
         for g in gates:
@@ -256,7 +259,10 @@ class Circuit:
         if name == "custom2":
             return check(self.lib.nqpu_circuit_add_custom_2q(self.h_, qs[0], qs[1], _cmat(matrix, 16)), name)
         fn = getattr(self.lib, _CIRC_FN[name])
-        check(fn(self.h_, *qs, *[float(p) for p in params]), name)
+        ps = [float(p) for p in tuple(params)[:NPARAMS[name]]]
+        if len(ps) != NPARAMS[name]:
+            raise ValueError(f"{name} takes {NPARAMS[name]} parameters")
+        check(fn(self.h_, *qs, *ps), name)
 
     def extend(self, gates):
         for g in gates:
@@ -274,7 +280,7 @@ class Circuit:
         return int(self.lib.nqpu_circuit_depth(self.h_))
 
     def plan_stats(self, num_qubits: int, dtype: str = "c128", mode: str = "tiled"):
-        out = (C.c_uint64 * 3)()
-        check(self.lib.nqpu_circuit_plan_stats(self.h_, int(num_qubits), DTYPES[dtype], MODES[mode], out, 3),
+        out = (C.c_uint64 * 4)()
+        check(self.lib.nqpu_circuit_plan_stats(self.h_, int(num_qubits), DTYPES[dtype], MODES[mode], out, 4),
               "plan_stats")
-        return {"passes": int(out[0]), "ops": int(out[1]), "stages": int(out[2])}
+        return {"passes": int(out[0]), "ops": int(out[1]), "stages": int(out[2]), "upload_bytes": int(out[3])}
