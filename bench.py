@@ -187,6 +187,8 @@ def run_engine(args):
     lib = _lib.load()
 
     n, depth = args.qubits, args.depth
+    if args.tile_ctas:
+        _lib.check(lib.nqpu_tile_config_set(1 if args.dtype == "c64" else 0, args.tile_ctas), "tile_config")
     gates = brickwork(n, depth, args.seed)
     G = len(gates)
     amp_bytes = 8 if args.dtype == "c64" else 16
@@ -331,6 +333,7 @@ def run_engine(args):
             "config": {"workload": f"brickwork {n}q depth {depth} {'complex64' if args.dtype == 'c64' else 'complex128'}",
                        "gates": G, "seed": args.seed, "engine_mode": args.mode,
                        "plan": {"passes": stats["passes"], "stages": stats["stages"]},
+                       "tile_ctas_per_sm": int(lib.nqpu_tile_config_get(1 if args.dtype == "c64" else 0)),
                        "l2": "state 8 GiB >> 126 MB L2; no flush", "parallelism": f"replicas{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clk,
@@ -355,6 +358,7 @@ def main():
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
     ap.add_argument("--mode", default="tiled", choices=["tiled", "pergate", "fused"])
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--tile-ctas", type=int, default=0, help="tiled kernel CTAs per SM (1 or 2; 0 = library default)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget-s", type=float, default=15.0)
     ap.add_argument("--ref-step-s", type=float, default=4.0)

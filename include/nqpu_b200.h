@@ -242,6 +242,11 @@ NqpuError    nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* stat
  * launch_ms[i] = device time of launch i (i < *count <= len). */
 NqpuError    nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,
                                   float* launch_ms, uint32_t len, uint32_t* count);
+/* Tiled-pass kernel configuration per dtype: ctas_per_sm = 1 (one CTA per SM,
+ * double-buffered tiles) or 2 (two CTAs per SM, single-buffered).  Set by the
+ * autotuner; applies to launches made after the call. */
+NqpuError    nqpu_tile_config_set(NqpuDtype dtype, uint32_t ctas_per_sm);
+uint32_t     nqpu_tile_config_get(NqpuDtype dtype);
 /* Plan statistics of the last execution of `circuit` in `mode` on an n-qubit state:
  * out[0] = HBM passes (kernel launches over the full state), out[1] = lowered ops,
  * out[2] = register stages (tiled) or fused unitaries (fused), out[3] (when

@@ -24,6 +24,10 @@ cudaError_t launch_pergate(DType dt, void* amp, int n, const Op& op, cudaStream_
 
 // --- tiled pass path ---------------------------------------------------------
 int tile_kmax_for(DType dt);
+// CTA configuration of the tiled pass kernel (1: one CTA/SM, double-buffered
+// tiles; 2: two CTAs/SM, single-buffered).
+void tile_config_set(DType dt, int minb);
+int tile_config_get(DType dt);
 cudaError_t launch_tile_pass(DType dt, void* amp, int n, const PassRec& host_pass,
                              const PassRec* d_passes, const StageRec* d_stages, const void* d_ops,
                              int pass_idx, cudaStream_t stream, int num_sms);

@@ -345,33 +345,83 @@ bool build_tile_plan(const std::vector<Op>& ops, int n, DType dt, int kmax, Tile
     P.stage_begin = int(out->stages.size());
 
     // ---- stages within the pass ----
+    // Virtual-index mask of a qubit read as a value (tile bit or ext bit).
+    auto vmask_of = [&](int q) -> uint32_t {
+      return tile_pos[q] >= 0 ? (1u << tile_pos[q]) : (1u << (k + ext_of_qubit[q]));
+    };
     std::vector<int> pending = taken;
     while (!pending.empty()) {
-      uint64_t R = 0;  // tile-bit mask of free register bits
-      uint64_t sblocked = 0;
-      std::vector<int> sops, srest;
+      uint64_t R = 0;          // tile-bit mask of free register bits
+      uint64_t no_reg = 0;     // tile bits that must stay thread-level in this stage
+      uint64_t sblocked = 0;   // qubits blocked for the rest of the stage
+      uint64_t perm_q = 0;     // qubits touched by deferred permutation ops
+      int n_cond = 0;
+      std::vector<int> sops, sdef, srest;
+      auto reg_tile_bit = [&](int q) -> int {  // tile bit of a register-capable qubit or -1
+        const int tb = tile_pos[q];
+        return tb;
+      };
       for (int idx : pending) {
         const Op& o = ops[idx];
         const uint64_t qm = o.qubit_mask();
         if (qm & sblocked) { sblocked |= qm; srest.push_back(idx); continue; }
         uint64_t need = 0;
         const uint64_t dt_ = dense_targets(o);
+        bool bad = false;
         for (int q = 0; q < n; ++q)
           if ((dt_ >> q) & 1) {
-            const int tb = tile_pos[q];
+            const int tb = reg_tile_bit(q);
             if (vb == 1 && tb == 0) continue;  // complex64: tile bit 0 is always in registers
+            if ((no_reg >> tb) & 1) bad = true;
             need |= 1ull << tb;
           }
-        if (popc(R | need) <= kRegFree) {
-          R |= need;
-          sops.push_back(idx);
-        } else {
+        const bool fits = !bad && popc(R | need) <= kRegFree;
+        // deferrable permutation: X/CNOT with <= 1 control, SWAP without controls
+        bool deferrable = false;
+        bool cond_ctrl = false;
+        if (fits && ((o.kind == OP_X1 && o.nctrl <= 1) || (o.kind == OP_SW && o.nctrl == 0))) {
+          deferrable = true;
+          auto on_bit0 = [&](int q) { return vb == 1 && tile_pos[q] == 0; };
+          if (o.kind == OP_X1 && o.nctrl == 1) {
+            const int cq = o.ctrl[0];
+            const int ctb = tile_pos[cq];
+            if (on_bit0(cq) || (ctb >= 0 && (((R | need) >> ctb) & 1))) {
+              cond_ctrl = false;  // register control
+            } else if (ctb >= 0 && !((no_reg >> ctb) & 1) && popc(R | need | (1ull << ctb)) <= kRegFree) {
+              need |= 1ull << ctb;  // room left: make the control a register bit
+              cond_ctrl = false;
+            } else {
+              cond_ctrl = true;  // thread-level control (only once the register set is full)
+            }
+            if (cond_ctrl && n_cond >= kMaxCondPerm) deferrable = false;
+          }
+        }
+        if (!fits || ((qm & perm_q) && !deferrable)) {
           sblocked |= qm;
           srest.push_back(idx);
+          continue;
+        }
+        R |= need;
+        if (deferrable) {
+          sdef.push_back(idx);
+          perm_q |= qm;
+          if (cond_ctrl) {
+            ++n_cond;
+            const int ctb = tile_pos[o.ctrl[0]];
+            if (ctb >= 0) no_reg |= 1ull << ctb;
+          }
+        } else {
+          sops.push_back(idx);
         }
       }
-      // fill R to exactly kRegFree tile bits (never tile bit 0 for complex64)
-      for (int tb = vb; tb < k && popc(R) < kRegFree; ++tb) R |= 1ull << tb;
+      // fill R to exactly kRegFree tile bits (never tile bit 0 for complex64,
+      // never a bit a deferred permutation reads as a thread-level control)
+      for (int tb = vb; tb < k && popc(R) < kRegFree; ++tb)
+        if (!((no_reg >> tb) & 1)) R |= 1ull << tb;
+      if (popc(R) != kRegFree) {
+        if (err) *err = "planner could not fill the register bits of a stage";
+        return false;
+      }
       StageRec S;
       std::memset(&S, 0, sizeof(S));
       int reg_of_tile[64];
@@ -381,6 +431,48 @@ bool build_tile_plan(const std::vector<Op>& ops, int n, DType dt, int kmax, Tile
         int j = 0;
         for (int tb = 0; tb < k; ++tb)
           if ((R >> tb) & 1) { S.rpos[j] = tb; reg_of_tile[tb] = vb + j; ++j; }
+      }
+      // compose the deferred permutations (in order) into pi = A p ^ b ^ conds
+      {
+        const int nr = vb + kRegFree;
+        int a[5], b = 0;
+        int cw[kMaxCondPerm];
+        uint32_t cc[kMaxCondPerm];
+        int nc = 0;
+        for (int j = 0; j < 5; ++j) a[j] = (j < nr) ? (1 << j) : 0;
+        auto apply_lin = [&](auto&& G) {
+          for (int j = 0; j < nr; ++j) a[j] = G(a[j]);
+          b = G(b);
+          for (int i = 0; i < nc; ++i) cw[i] = G(cw[i]);
+        };
+        for (int idx : sdef) {
+          const Op& o = ops[idx];
+          const int t = reg_of_tile[tile_pos[o.t0]];
+          if (o.kind == OP_SW) {
+            const int u = reg_of_tile[tile_pos[o.t1]];
+            apply_lin([&](int v) {
+              const int bt = (v >> t) & 1, bu = (v >> u) & 1;
+              return (v & ~((1 << t) | (1 << u))) | (bt << u) | (bu << t);
+            });
+          } else if (o.nctrl == 0) {
+            b ^= 1 << t;
+          } else {
+            const int cq = o.ctrl[0];
+            const int ctb = tile_pos[cq];
+            if (ctb >= 0 && reg_of_tile[ctb] >= 0) {
+              const int c = reg_of_tile[ctb];
+              apply_lin([&](int v) { return v ^ (((v >> c) & 1) << t); });
+            } else {
+              cc[nc] = vmask_of(cq);
+              cw[nc] = 1 << t;
+              ++nc;
+            }
+          }
+        }
+        for (int j = 0; j < 5; ++j) S.scol[j] = a[j];
+        S.sbx = b;
+        S.ncond = nc;
+        for (int i = 0; i < nc; ++i) { S.cond_cnr[i] = cc[i]; S.cond_w[i] = cw[i]; }
       }
       // thread-index bits: the non-register vector bits; the three lowest
       // thread bits take vector bits of distinct residue mod 3 when possible.
@@ -414,6 +506,31 @@ bool build_tile_plan(const std::vector<Op>& ops, int n, DType dt, int kmax, Tile
       return false;
     }
     remaining.swap(rest);
+  }
+  // Validate every table entry the kernel turns into a shift or an index.
+  for (const PassRec& P : out->passes) {
+    if (P.k < vb + kRegFree || P.k > kmax || P.c < 1 || P.c > P.k || P.k - P.c > 10 ||
+        P.n_out != n - P.k || P.k + P.n_ext > 32) {
+      if (err) *err = "invalid pass record";
+      return false;
+    }
+    for (int si = P.stage_begin; si < P.stage_end; ++si) {
+      const StageRec& S = out->stages[si];
+      uint32_t used = 0;
+      for (int j = 0; j < kRegFree; ++j) {
+        if (S.rpos[j] < vb || S.rpos[j] >= P.k) { if (err) *err = "invalid register bit"; return false; }
+        used |= 1u << (S.rpos[j] - vb);
+      }
+      if (S.n_tbits != P.k - vb - kRegFree) { if (err) *err = "invalid thread bits"; return false; }
+      for (int j = 0; j < S.n_tbits; ++j) {
+        if (S.tpos[j] < 0 || S.tpos[j] >= P.k - vb || ((used >> S.tpos[j]) & 1)) {
+          if (err) *err = "invalid thread bit position";
+          return false;
+        }
+        used |= 1u << S.tpos[j];
+      }
+      if (S.ncond < 0 || S.ncond > kMaxCondPerm) { if (err) *err = "invalid stage map"; return false; }
+    }
   }
   out->stats.passes = out->passes.size();
   out->stats.ops = ops.size();

@@ -96,12 +96,27 @@ struct PassRec {
   int32_t pad[2];
 };
 
+// Permutation ops (X, CNOT with at most one control, SWAP) are not executed in
+// registers: the planner composes them into an affine map over the register
+// index bits, pi(p) = A p ^ b ^ (conditional translations), and the stage's
+// write-back stores register p at the shared-memory slot of logical index
+// pi(p).  scol[j] = A e_j (mask over register bits); sbx = static b;
+// conditional translation i applies w = cond_w[i] when the amplitude's virtual
+// index has all bits cond_cnr[i] set (a control outside the register bits).
+constexpr int kMaxCondPerm = 4;
+
 struct StageRec {
   int32_t rpos[kRegFree];    // tile-local bit positions of the free register bits
   int32_t n_tbits;           // thread-index bits in use
   int32_t tpos[24];          // tile-local VECTOR bit position of thread-index bit j
   int32_t op_begin, op_end;  // range in the op table
   int32_t pad;
+  int32_t scol[5];
+  int32_t sbx;
+  int32_t ncond;
+  uint32_t cond_cnr[kMaxCondPerm];
+  int32_t cond_w[kMaxCondPerm];
+  int32_t pad2;
 };
 
 // Device op of a stage.  Register-bit numbering: complex64 register bit 0 is
