@@ -600,6 +600,8 @@ extern "C" NqpuError nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuSta
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;  // c_ffi.rs:1360
   if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED)
     return NQPU_INVALID_PARAMETER;
+  // the fused mode runs complex64 states of >= 12 qubits (5 fused + 7 group bits)
+  if (mode == NQPU_MODE_FUSED && (s->dt != DType::C64 || s->n < 12)) return NQPU_INVALID_PARAMETER;
   cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode));
   if (e != cudaSuccess) return map_cuda(e);
   NQ_TRY(cudaStreamSynchronize(s->stream));
@@ -612,6 +614,7 @@ extern "C" NqpuError nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState*
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;
+  if (mode == NQPU_MODE_FUSED && (s->dt != DType::C64 || s->n < 12)) return NQPU_INVALID_PARAMETER;
   std::vector<cudaEvent_t> ev;
   cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode), &ev);
   cudaError_t e2 = cudaStreamSynchronize(s->stream);

@@ -320,7 +320,11 @@ cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cuda
     }
     return cudaSuccess;
   }
-  if (effective == NQPU_MODE_FUSED) return fused_run(p->fused, s, events);
+  if (effective == NQPU_MODE_FUSED) {
+    e = fused_run(p->fused, s, events);
+    if (e != cudaSuccess) return e;
+    return fused_check_error(p->fused, s->stream);  // bounded-wait expiry flag
+  }
   for (size_t i = 0; i < p->tile.passes.size(); ++i) {
     e = launch_tile_pass(s->dt, s->amp, int(s->n), p->tile.passes[i], p->d_passes, p->d_stages,
                          p->d_ops, int(i), s->stream, device_sms());

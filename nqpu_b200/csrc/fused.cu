@@ -1,8 +1,444 @@
-#include "fused.h"
+// Fused execution mode (precision form).
+//
+// Host: a fusion pass packs runs of gates into dense <=5-qubit unitaries.  It
+// generalises the reference's fuse_gates (circuits/synthesis/gate_fusion.rs:537:
+// 1q runs -> 2x2, absorption into 2q gates -> 4x4) from 2 to 5 qubits: ops are
+// taken greedily in circuit order while the union of their qubits stays within
+// 5, and an op may move ahead of a deferred op only when they share no qubit.
+// Each cluster's 32x32 unitary is accumulated in FP64 by applying the cluster's
+// ops to the 32 basis columns.
+//
+// Device: one launch per fused unitary U on qubits F = (f0 < ... < f4).  The
+// state is viewed as groups of 32 amplitudes (the F-subspace of a fixed
+// assignment of the other qubits).  A CTA takes 128 groups at a time and
+// computes out_g = U v_g for all of them as one tensor-core GEMM on the real
+// embedding:  D[128 x 64] = A[128 x 64] * B^T, A row g = (re, im) of the 32
+// amplitudes of group g, B = R (64 x 64 real form of U).  Inputs are split
+// into TF32 hi/lo parts (hi = x rounded to TF32, lo = the remainder rounded to
+// TF32) and D = A_hi B_hi + A_hi B_lo + A_lo B_hi is accumulated in FP32 in
+// tensor memory by tcgen05.mma kind::tf32 (24 MMAs of 128x64x8 per tile).
+// Operands live in shared memory in the K-major 128-byte-swizzled layout.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
 #include "engine.h"
+#include "fused.h"
+#include "fusion.h"
+#include "kernels.h"
+#include "sv_device.cuh"
+
 namespace nqpu {
-bool fused_plan_build(const std::vector<Op>&, int, DType, void** plan, PlanStats*) { *plan = nullptr; return false; }
-bool fused_plan_stats(const std::vector<Op>&, int, DType, PlanStats*) { return false; }
-void fused_plan_free(void*) {}
-cudaError_t fused_run(void*, StateImpl*, std::vector<cudaEvent_t>*) { return cudaErrorNotSupported; }
+
+// ---------------------------------------------------------------------------
+// Device kernel
+// ---------------------------------------------------------------------------
+constexpr int kFusedThreads = 128;         // one thread per group row (M = 128)
+constexpr int kRowBytes = 256;             // 64 fp32 per row
+constexpr int kAtomBytes = 128 * 128;      // one K-atom (32 tf32) of 128 rows
+constexpr int kAPlane = 2 * kAtomBytes;    // 32 KB: 128 rows x 64 tf32
+constexpr int kBPlane = 2 * 64 * 128;      // 16 KB: 64 rows x 64 tf32
+constexpr int kSmemFused = 2 * kAPlane + 2 * kBPlane + 1024 /*align*/ + 2048 /*tables*/;
+constexpr uint32_t kWaitLimit = 1u << 22;  // bounded mbarrier wait (iterations)
+
+struct FusedArgs {
+  int n;
+  int q[5];               // fused qubits ascending
+  int gq[7];              // group bits: the 7 lowest qubits outside F (or fewer when n < 12)
+  int ng;                 // number of group bits used
+  int n_out;              // tile-id bits
+  int qout[kMaxQubits];   // qubits of tile-id bits
+  int lane_over_j;        // 1: F contains qubit 0 (warp loads a group's amplitudes)
+};
+
+// Byte offset of element (row r, fp32 column k) in a K-major SW128 operand of
+// `rows` rows: K-atom (32 fp32 = 128 B per row) stride rows * 128 B, 8-row
+// groups at 1024 B, 16-byte chunks XOR-swizzled with the row within the group.
+template <uint32_t kRows>
+__device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t k) {
+  const uint32_t atom = k >> 5;
+  const uint32_t byte = (k & 31) * 4;
+  const uint32_t chunk = byte >> 4, within = byte & 15;
+  return atom * (kRows * 128u) + (r >> 3) * 1024 + (r & 7) * 128 + ((chunk ^ (r & 7)) << 4) + within;
+}
+
+// Round-to-nearest TF32 (10 explicit mantissa bits): with hi = rn(x) and
+// lo = rn(x - hi), |x - hi - lo| <= 2^-24 |x| and the tensor core reads both
+// parts exactly.
+__device__ __forceinline__ float tf32_rn(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  // K-major, SWIZZLE_128B, SBO = 1024 B between 8-row groups, LBO unused (1),
+  // version 1 (sm_100), start address >> 4.
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFF);
+  d |= uint64_t(1) << 16;
+  d |= uint64_t((1024 >> 4) & 0x3FFF) << 32;
+  d |= uint64_t(1) << 46;
+  d |= uint64_t(2) << 61;
+  return d;
+}
+
+// kind::tf32, D fp32, A/B tf32, both K-major, N = 64, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(addr), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(addr), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// Renormalisation: every launch writes the FP64 sum of |out|^2 of the tiles it
+// processed to out_norm[blockIdx.x]; the next launch sums those partials (in a
+// fixed order) and scales its own output by 1/sqrt(sum), so the norm drift of
+// each fused unitary is removed by the next one at no extra HBM pass.
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    k_fused_apply(float* __restrict__ amp, FusedArgs A, const float* __restrict__ bmat /* hi[64][64], lo[64][64] */,
+                  const double* __restrict__ prev_norm, int n_prev, double* __restrict__ out_norm,
+                  uint64_t n_tiles, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-aligned operand region
+  const uint32_t raw_s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_raw));
+  const uint32_t pad = (1024 - (raw_s & 1023)) & 1023;
+  unsigned char* base = smem_raw + pad;
+  unsigned char* a_hi = base;
+  unsigned char* a_lo = base + kAPlane;
+  unsigned char* b_hi = base + 2 * kAPlane;
+  unsigned char* b_lo = b_hi + kBPlane;
+  uint64_t* gofs = reinterpret_cast<uint64_t*>(b_lo + kBPlane);   // 128 entries
+  uint64_t* fofs = gofs + 128;                                    // 32 entries
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_holder;
+  __shared__ int abort_flag;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t mbar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar));
+
+  // offset tables
+  if (tid < 128) {
+    uint64_t o = 0;
+    for (int b = 0; b < A.ng; ++b)
+      if ((tid >> b) & 1) o |= 1ull << A.gq[b];
+    gofs[tid] = o;
+  }
+  if (tid < 32) {
+    uint64_t o = 0;
+    for (int b = 0; b < 5; ++b)
+      if ((tid >> b) & 1) o |= 1ull << A.q[b];
+    fofs[tid] = o;
+  }
+  // B operand (constant for the launch): row n (output real index), col k
+  for (int i = tid; i < 64 * 64; i += blockDim.x) {
+    const uint32_t r = i >> 6, k = i & 63;
+    *reinterpret_cast<float*>(b_hi + sw128_off<64>(r, k)) = __ldg(bmat + i);
+    *reinterpret_cast<float*>(b_lo + sw128_off<64>(r, k)) = __ldg(bmat + 4096 + i);
+  }
+  if (tid == 0) {
+    mbar_init(mbar_addr, 1);
+    abort_flag = 0;
+  }
+  if (warp == 0) {
+    const uint32_t holder = static_cast<uint32_t>(__cvta_generic_to_shared(&tmem_holder));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(holder), "r"(64));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_holder;
+  float scale = 1.0f;
+  if (prev_norm) {
+    double tot = 0.0;
+    for (int i = 0; i < n_prev; ++i) tot += prev_norm[i];
+    scale = tot > 0.0 ? float(1.0 / sqrt(tot)) : 1.0f;
+  }
+  double norm_acc = 0.0;
+
+  const uint32_t ahi_s = static_cast<uint32_t>(__cvta_generic_to_shared(a_hi));
+  const uint32_t alo_s = static_cast<uint32_t>(__cvta_generic_to_shared(a_lo));
+  const uint32_t bhi_s = static_cast<uint32_t>(__cvta_generic_to_shared(b_hi));
+  const uint32_t blo_s = static_cast<uint32_t>(__cvta_generic_to_shared(b_lo));
+
+  uint32_t phase = 0;
+  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    uint64_t tb = 0;
+    for (int j = 0; j < A.n_out; ++j)
+      if ((tile >> j) & 1ull) tb |= 1ull << A.qout[j];
+    const float2* src = reinterpret_cast<const float2*>(amp) + tb;
+
+    // HBM -> A_hi / A_lo (split), swizzled K-major rows
+    auto put = [&](uint32_t row, uint32_t j, float2 v) {
+      const uint32_t o0 = sw128_off<128>(row, 2 * j), o1 = sw128_off<128>(row, 2 * j + 1);
+      const float hr = tf32_rn(v.x), hi_ = tf32_rn(v.y);
+      *reinterpret_cast<float*>(a_hi + o0) = hr;
+      *reinterpret_cast<float*>(a_hi + o1) = hi_;
+      *reinterpret_cast<float*>(a_lo + o0) = tf32_rn(v.x - hr);
+      *reinterpret_cast<float*>(a_lo + o1) = tf32_rn(v.y - hi_);
+    };
+    if (A.lane_over_j) {
+      // a warp reads the 32 amplitudes of one group per step (qubit 0 is in F)
+      for (int g = warp; g < 128; g += kFusedThreads / 32) put(g, lane, __ldcs(src + gofs[g] + fofs[lane]));
+    } else {
+      float2 v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __ldcs(src + gofs[tid] + fofs[j]);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) put(tid, j, v[j]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+    if (tid == 0) {
+      uint32_t acc = 0;
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk) {
+        const uint32_t off = (kk >> 2) * kAtomBytes + (kk & 3) * 32;
+        const uint32_t boff = (kk >> 2) * (64 * 128) + (kk & 3) * 32;
+        mma_tf32(tmem, umma_desc(ahi_s + off), umma_desc(bhi_s + boff), acc);
+        acc = 1;
+        mma_tf32(tmem, umma_desc(ahi_s + off), umma_desc(blo_s + boff), 1);
+        mma_tf32(tmem, umma_desc(alo_s + off), umma_desc(bhi_s + boff), 1);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_addr)
+                   : "memory");
+    }
+    // bounded wait for the MMAs
+    {
+      uint32_t it = 0;
+      bool done = false;
+      while (!(done = mbar_try_wait(mbar_addr, phase)) && ++it < kWaitLimit) {
+      }
+      if (!done) {
+        atomicExch(err, 1);
+        abort_flag = 1;
+      }
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+    // TMEM -> registers: warp w reads lanes 32w..32w+31, thread = row
+    uint32_t r[64];
+    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+
+    float2* dst = reinterpret_cast<float2*>(amp) + tb + gofs[tid];
+    double tile_norm = 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float2 o = make_float2(__uint_as_float(r[2 * j]) * scale, __uint_as_float(r[2 * j + 1]) * scale);
+      tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+      __stcs(dst + fofs[j], o);
+    }
+    norm_acc += tile_norm;
+
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();  // TMEM and the A planes are reused by the next tile
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  }
+  // per-CTA FP64 norm partial (fixed-order tree: warp shuffles, then warp 0)
+  __shared__ double wsum[kFusedThreads / 32];
+  double v = norm_acc;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) wsum[warp] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kFusedThreads / 32; ++w) t += wsum[w];
+    out_norm[blockIdx.x] = t;
+  }
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64));
+}
+
+// ---------------------------------------------------------------------------
+// Plan management
+// ---------------------------------------------------------------------------
+struct FusedPlanImpl {
+  int n = 0;
+  std::vector<FusedGate> gates;
+  std::vector<FusedArgs> args;
+  float* d_bmats = nullptr;  // per gate: hi[64][64], lo[64][64]
+  double* d_norm = nullptr;  // two buffers of per-CTA norm partials (ping-pong)
+  int norm_slots = 0;
+  int* d_err = nullptr;
+};
+
+static void real_embedding(const FusedGate& g, float* hi, float* lo) {
+  for (int j = 0; j < 32; ++j)
+    for (int k = 0; k < 32; ++k) {
+      const cplx u = g.u[j * 32 + k];
+      const double vals[2][2] = {{u.real(), -u.imag()}, {u.imag(), u.real()}};
+      auto rn = [](float x) {
+        uint32_t bits;
+        std::memcpy(&bits, &x, 4);
+        bits = (bits + 0x1000u) & 0xFFFFE000u;
+        float h;
+        std::memcpy(&h, &bits, 4);
+        return h;
+      };
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          const float h = rn(float(vals[a][b]));
+          const int row = 2 * j + a, col = 2 * k + b;
+          hi[row * 64 + col] = h;
+          lo[row * 64 + col] = rn(float(vals[a][b] - double(h)));
+        }
+    }
+}
+
+static FusedArgs make_args(const FusedGate& g, int n) {
+  FusedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = n;
+  uint64_t F = 0;
+  for (int i = 0; i < 5; ++i) { a.q[i] = g.q[i]; F |= 1ull << g.q[i]; }
+  int ng = 0;
+  uint64_t G = 0;
+  for (int q = 0; q < n && ng < 7; ++q)
+    if (!((F >> q) & 1)) { a.gq[ng++] = q; G |= 1ull << q; }
+  a.ng = ng;
+  int no = 0;
+  for (int q = 0; q < n; ++q)
+    if (!(((F | G) >> q) & 1)) a.qout[no++] = q;
+  a.n_out = no;
+  a.lane_over_j = (F & 1ull) ? 1 : 0;
+  return a;
+}
+
+bool fused_plan_stats(const std::vector<Op>& ops, int n, DType dt, PlanStats* stats) {
+  if (dt != DType::C64 || n < 12) return false;
+  std::vector<FusedGate> g = fuse_ops(ops, n);
+  stats->passes = g.size();
+  stats->ops = ops.size();
+  stats->stages = g.size();
+  stats->upload_bytes = g.size() * 2 * 64 * 64 * sizeof(float);
+  return true;
+}
+
+bool fused_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, PlanStats* stats) {
+  *plan = nullptr;
+  // complex64 only; 12 qubits minimum (5 fused + 7 group bits per 128-row tile)
+  if (dt != DType::C64 || n < 12) return false;
+  auto* p = new FusedPlanImpl();
+  p->n = n;
+  p->gates = fuse_ops(ops, n);
+  const size_t G = p->gates.size();
+  std::vector<float> host(std::max<size_t>(1, G) * 2 * 4096);
+  for (size_t i = 0; i < G; ++i) {
+    real_embedding(p->gates[i], host.data() + i * 8192, host.data() + i * 8192 + 4096);
+    p->args.push_back(make_args(p->gates[i], n));
+  }
+  bool ok = cudaMalloc(reinterpret_cast<void**>(&p->d_bmats), host.size() * sizeof(float)) == cudaSuccess;
+  ok = ok && cudaMemcpy(p->d_bmats, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess;
+  p->norm_slots = device_sms();
+  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_norm), sizeof(double) * 2 * p->norm_slots) == cudaSuccess;
+  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_err), sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMemset(p->d_err, 0, sizeof(int)) == cudaSuccess;
+  if (!ok) {
+    fused_plan_free(p);
+    return false;
+  }
+  stats->passes = G;
+  stats->ops = ops.size();
+  stats->stages = G;
+  stats->upload_bytes = host.size() * sizeof(float);
+  *plan = p;
+  return true;
+}
+
+void fused_plan_free(void* plan) {
+  auto* p = static_cast<FusedPlanImpl*>(plan);
+  if (!p) return;
+  if (p->d_bmats) cudaFree(p->d_bmats);
+  if (p->d_norm) cudaFree(p->d_norm);
+  if (p->d_err) cudaFree(p->d_err);
+  delete p;
+}
+
+cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
+  auto* p = static_cast<FusedPlanImpl*>(plan);
+  if (!p || s->dt != DType::C64 || int(s->n) != p->n) return cudaErrorInvalidValue;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_fused_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFused);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int n = p->n;
+  const uint64_t n_tiles = 1ull << (n - 12);
+  const unsigned grid = unsigned(std::min<uint64_t>(n_tiles, uint64_t(p->norm_slots)));
+  cudaError_t e = cudaSuccess;
+  int prev_grid = 0;
+  for (size_t i = 0; i < p->gates.size(); ++i) {
+    double* outn = p->d_norm + (i & 1) * p->norm_slots;
+    const double* prevn = i ? p->d_norm + ((i + 1) & 1) * p->norm_slots : nullptr;
+    k_fused_apply<<<grid, kFusedThreads, kSmemFused, s->stream>>>(
+        static_cast<float*>(s->amp), p->args[i], p->d_bmats + i * 8192, prevn, prev_grid, outn, n_tiles,
+        p->d_err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    prev_grid = int(grid);
+    if (events) {
+      cudaEvent_t ev;
+      if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+      events->push_back(ev);
+      if ((e = cudaEventRecord(ev, s->stream)) != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+cudaError_t fused_check_error(void* plan, cudaStream_t st) {
+  auto* p = static_cast<FusedPlanImpl*>(plan);
+  if (!p) return cudaSuccess;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  return h ? cudaErrorLaunchTimeout : cudaSuccess;
+}
+
 }  // namespace nqpu

@@ -11,4 +11,6 @@ bool fused_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, 
 bool fused_plan_stats(const std::vector<Op>& ops, int n, DType dt, PlanStats* stats);
 void fused_plan_free(void* plan);
 cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events);
+// Reads the plan's device error flag (set when a bounded wait expired).
+cudaError_t fused_check_error(void* plan, cudaStream_t st);
 }  // namespace nqpu

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "planner.h"
+#include "fusion.h"
 
 using namespace nqpu;
 using cd = std::complex<double>;
@@ -201,4 +202,49 @@ extern "C" int emu_run(int n, int c64, const double* flat, int ngates, double* s
   else run_plan<double>(plan, st);
   for (size_t i = 0; i < st.size(); ++i) { state[2 * i] = st[i].real(); state[2 * i + 1] = st[i].imag(); }
   return int(plan.passes.size());
+}
+
+// Fusion pass check: apply the fused 32x32 unitaries in FP64.  Returns the
+// number of fused unitaries.
+extern "C" int emu_fused(int n, const double* flat, int ngates, double* state) {
+  std::vector<GateRec> gates(ngates);
+  for (int i = 0; i < ngates; ++i) {
+    const double* g = flat + size_t(i) * 40;
+    GateRec& r = gates[i];
+    r.code = uint8_t(g[0]);
+    r.nq = uint8_t(gate_arity(r.code));
+    for (int j = 0; j < 3; ++j) r.q[j] = int(g[1 + j]);
+    for (int j = 0; j < 4; ++j) r.p[j] = g[4 + j];
+    for (int j = 0; j < 16; ++j) r.m[j] = cplx(g[8 + 2 * j], g[9 + 2 * j]);
+  }
+  const std::vector<FusedGate> fg = fuse_ops(lower_circuit(gates), n);
+  const size_t dim = size_t(1) << n;
+  std::vector<cd> st(dim);
+  for (size_t i = 0; i < dim; ++i) st[i] = cd(state[2 * i], state[2 * i + 1]);
+  for (const FusedGate& f : fg) {
+    uint64_t fm = 0;
+    for (int b = 0; b < 5; ++b) fm |= 1ull << f.q[b];
+    for (size_t base = 0; base < dim; ++base) {
+      if (base & fm) continue;
+      cd v[32], w[32];
+      for (int j = 0; j < 32; ++j) {
+        size_t idx = base;
+        for (int b = 0; b < 5; ++b)
+          if ((j >> b) & 1) idx |= size_t(1) << f.q[b];
+        v[j] = st[idx];
+      }
+      for (int r = 0; r < 32; ++r) {
+        w[r] = 0;
+        for (int c = 0; c < 32; ++c) w[r] += f.u[r * 32 + c] * v[c];
+      }
+      for (int j = 0; j < 32; ++j) {
+        size_t idx = base;
+        for (int b = 0; b < 5; ++b)
+          if ((j >> b) & 1) idx |= size_t(1) << f.q[b];
+        st[idx] = w[j];
+      }
+    }
+  }
+  for (size_t i = 0; i < dim; ++i) { state[2 * i] = st[i].real(); state[2 * i + 1] = st[i].imag(); }
+  return int(fg.size());
 }

@@ -19,13 +19,17 @@ SO = ROOT / "tests" / "_build" / "libplanemu.so"
 @pytest.fixture(scope="module")
 def emu():
     SO.parent.mkdir(exist_ok=True)
-    srcs = [ROOT / "tests" / "plan_emulator.cpp", ROOT / "nqpu_b200" / "csrc" / "planner.cpp"]
-    if not SO.exists() or SO.stat().st_mtime < max(s.stat().st_mtime for s in srcs + [ROOT / "nqpu_b200" / "csrc" / "sv_types.h"]):
+    srcs = [ROOT / "tests" / "plan_emulator.cpp", ROOT / "nqpu_b200" / "csrc" / "planner.cpp",
+            ROOT / "nqpu_b200" / "csrc" / "fusion.cpp"]
+    deps = srcs + [ROOT / "nqpu_b200" / "csrc" / h for h in ("sv_types.h", "planner.h", "fusion.h")]
+    if not SO.exists() or SO.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", str(ROOT / "nqpu_b200" / "csrc"),
                         *map(str, srcs), "-o", str(SO)], check=True)
     lib = C.CDLL(str(SO))
     lib.emu_run.restype = C.c_int
     lib.emu_run.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]
+    lib.emu_fused.restype = C.c_int
+    lib.emu_fused.argtypes = [C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]
     return lib
 
 
@@ -103,3 +107,59 @@ def test_emulated_plan_many_seeds_small(emu, c64, n):
         o = OracleState(n)
         o.apply(gates)
         assert 1 - fid(got, o.amplitudes()) <= (1e-6 if c64 else 1e-12), (seed, n, c64)
+
+
+def run_fused(lib, n, gates):
+    flat = np.ascontiguousarray(circuits.flatten(gates))
+    st = np.zeros(2 << n)
+    st[0] = 1.0
+    nf = lib.emu_fused(n, flat.ctypes.data_as(C.POINTER(C.c_double)), len(flat), st.ctypes.data_as(C.POINTER(C.c_double)))
+    return st.view(np.complex128), nf
+
+
+@pytest.mark.parametrize("n", [5, 6, 9, 12])
+def test_fusion_pass_matches_oracle(emu, n):
+    rng = np.random.default_rng(77 + n)
+    gates = random_circuit(rng, n, 12 * n)
+    got, nf = run_fused(emu, n, gates)
+    o = OracleState(n)
+    o.apply(gates)
+    assert 1 - fid(got, o.amplitudes()) <= 1e-12
+    assert nf < len(gates)
+
+
+def test_fusion_pass_tfim_cluster_sizes(emu):
+    n = 12
+    gates, _ = circuits.tfim_trotter(n, 10, seed=3)
+    o = OracleState(n)
+    o.set_basis(circuits.neel_index(n))
+    o.apply(gates)
+    flat = np.ascontiguousarray(circuits.flatten(gates))
+    st = np.zeros(2 << n)
+    st[2 * circuits.neel_index(n)] = 1.0
+    nf = emu.emu_fused(n, flat.ctypes.data_as(C.POINTER(C.c_double)), len(flat), st.ctypes.data_as(C.POINTER(C.c_double)))
+    assert 1 - fid(st.view(np.complex128), o.amplitudes()) <= 1e-12
+    assert len(gates) / nf >= 4  # several gates per fused unitary
+
+
+def test_split_tf32_product_accuracy():
+    """The split-TF32 product used on the tensor cores (hi*hi + hi*lo + lo*hi,
+    FP32 accumulation) keeps the relative error of a 64-term dot product near
+    FP32 level, far below plain TF32."""
+    rng = np.random.default_rng(1)
+
+    def tf32(x):  # round to nearest, as the kernel splits
+        b = np.asarray(x, np.float32).view(np.uint32)
+        return ((b + np.uint32(0x1000)) & np.uint32(0xFFFFE000)).view(np.float32)
+
+    a = rng.normal(size=(256, 64)).astype(np.float32)
+    b = rng.normal(size=(64, 64)).astype(np.float32)
+    ah, bh = tf32(a), tf32(b)
+    al, bl = tf32(a - ah), tf32(b - bh)
+    exact = a.astype(np.float64) @ b.astype(np.float64).T
+    split = (ah.astype(np.float64) @ bh.T.astype(np.float64) + ah.astype(np.float64) @ bl.T.astype(np.float64)
+             + al.astype(np.float64) @ bh.T.astype(np.float64))
+    plain = ah.astype(np.float64) @ bh.T.astype(np.float64)
+    rel = lambda x: np.abs(x - exact).max() / np.abs(exact).max()
+    assert rel(split) < 5e-7
+    assert rel(plain) > 20 * rel(split)
