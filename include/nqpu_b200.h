@@ -234,6 +234,23 @@ NqpuError    nqpu_circuit_add_cu(NqpuCircuit* c, uint32_t control, uint32_t targ
 NqpuError    nqpu_circuit_add_custom_1q(NqpuCircuit* c, uint32_t q, const NqpuComplex* matrix);
 /* nqpu_gate_custom_2q convention: q1 is the HIGH bit of the sub-index. */
 NqpuError    nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uint32_t q2, const NqpuComplex* matrix);
+/* No counterpart in the reference.  All <Z_i> (FP64) of a state that lives in
+ * the CALLER's device memory, for callers that cannot allocate device memory:
+ * code running while a stream is captured into a CUDA graph, plugins whose
+ * host runtime owns the device memory pool, real-time loops that must not wait
+ * on the allocator.  It allocates nothing: the reduction's scratch is a fixed
+ * array in this library's device module (about 2.2 MB on every GPU that loads
+ * the library, kept until exit).  d_amplitudes: 2^n interleaved (re, im)
+ * amplitudes of `dtype`, 16-byte aligned; d_out: n doubles in device memory;
+ * cuda_stream: a cudaStream_t (NULL = legacy default stream).  The work is only
+ * queued; synchronise the stream before reading d_out.  Limit: complex64 states
+ * up to 28 qubits, complex128 up to 27; larger states return
+ * NQPU_INVALID_PARAMETER.  The first call on a device resolves the scratch
+ * address and should come before any stream capture.  Calls share the scratch,
+ * so calls whose kernels overlap on the GPU race. */
+NqpuError   nqpu_expectation_z_all_noalloc(const void* d_amplitudes, uint32_t num_qubits,
+                                           NqpuDtype dtype, double* d_out, void* cuda_stream);
+
 /* Like nqpu_circuit_create with the 34-qubit engine limit. */
 NqpuCircuit* nqpu_circuit_create_ex(uint32_t num_qubits);
 /* Run with an explicit engine mode. */
