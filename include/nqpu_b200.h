@@ -271,6 +271,34 @@ uint32_t     nqpu_tile_config_get(NqpuDtype dtype);
 NqpuError    nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_t num_qubits,
                                      NqpuDtype dtype, NqpuMode mode, uint64_t* out, uint32_t len);
 
+/* ------------------------------------------------------------------ */
+/* Batched execution (no counterpart in the reference): many circuits   */
+/* of different sizes in one persistent, graph-captured launch; each    */
+/* circuit returns <H> of its own 1D Ising Hamiltonian                  */
+/* H = sum_i J_i Z_i Z_{i+1} + sum_i h_i X_i (complex64 states).        */
+/* ------------------------------------------------------------------ */
+typedef struct NqpuBatch NqpuBatch;
+typedef enum {
+    NQPU_BATCH_SMALL_MAX_QUBITS = 0, /* circuits up to this size run in one CTA's shared memory (5..13) */
+    NQPU_BATCH_TILE_QUBITS      = 1, /* tile bits of the larger circuits' passes (10..13) */
+    NQPU_BATCH_QUEUE_ORDER      = 2, /* 0: small circuits between pass rounds, 1: first, 2: last */
+    NQPU_BATCH_CTAS_PER_SM      = 3  /* persistent CTAs per SM (1..2) */
+} NqpuBatchParam;
+
+NqpuBatch*  nqpu_batch_create(void);
+void        nqpu_batch_destroy(NqpuBatch* batch);
+/* Append a circuit (5..24 qubits; the gate list is copied) with J[n-1], h[n]. */
+NqpuError   nqpu_batch_add_ising(NqpuBatch* batch, const NqpuCircuit* circuit, const double* J,
+                                 const double* h, uint32_t* index);
+NqpuError   nqpu_batch_config(NqpuBatch* batch, NqpuBatchParam param, int32_t value);
+/* Plan every circuit, upload the task queue and capture the CUDA graph
+ * (run() does it on first use). */
+NqpuError   nqpu_batch_prepare(NqpuBatch* batch);
+/* Replay the graph; results[i] = <H> of circuit i (FP64).  len >= circuits. */
+NqpuError   nqpu_batch_run(NqpuBatch* batch, double* results, uint32_t len);
+/* out[0..4] = circuits, small circuits, tasks, HBM arena bytes, tiled passes. */
+NqpuError   nqpu_batch_stats(const NqpuBatch* batch, uint64_t* out, uint32_t len);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -39,6 +39,8 @@ _SCALARS = {
     "NqpuError": C.c_int,
     "NqpuDtype": C.c_int,
     "NqpuMode": C.c_int,
+    "NqpuBatchParam": C.c_int,
+    "int32_t": C.c_int32,
     "NqpuComplex": NqpuComplex,
     "NqpuVersion": NqpuVersion,
     "NqpuMeasurement": NqpuMeasurement,

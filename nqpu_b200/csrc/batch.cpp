@@ -1,0 +1,313 @@
+// Host side of batched execution: per-circuit tiled plans, the dependency-
+// ordered task queue, the HBM state arena, and a captured CUDA graph that
+// resets the queue, runs the persistent kernel and copies the results back.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/nqpu_b200.h"
+#include "batch.h"
+#include "engine.h"
+#include "kernels.h"
+#include "planner.h"
+
+namespace nqpu {
+
+struct BatchEntry {
+  int n = 0;
+  std::vector<GateRec> gates;
+  std::vector<double> J, h;
+};
+
+struct BatchImpl {
+  std::vector<BatchEntry> entries;
+  int small_max = 13;    // circuits up to this size run in one CTA's shared memory
+  int plan_kmax = 13;    // tile bits of the larger circuits' passes
+  int order = 0;         // queue order strategy
+  int ctas_per_sm = 2;
+  bool built = false;
+  cudaStream_t stream = nullptr;
+  float* d_arena = nullptr;
+  BatchCirc* d_circs = nullptr;
+  BatchTask* d_tasks = nullptr;
+  PassRec* d_passes = nullptr;
+  StageRec* d_stages = nullptr;
+  TileOp<float>* d_ops = nullptr;
+  double* d_obs = nullptr;
+  uint32_t* d_counters = nullptr;
+  double* d_partials = nullptr;
+  double* d_results = nullptr;
+  uint32_t* d_cursor = nullptr;
+  int* d_err = nullptr;
+  double* h_results = nullptr;
+  int* h_err = nullptr;
+  uint32_t n_tasks = 0, n_counters = 0;
+  size_t arena_bytes = 0, n_small = 0, n_passes_total = 0;
+  cudaGraphExec_t graph = nullptr;
+};
+
+static void batch_release(BatchImpl* b) {
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  void* ptrs[] = {b->d_arena, b->d_circs, b->d_tasks, b->d_passes, b->d_stages, b->d_ops, b->d_obs,
+                  b->d_counters, b->d_partials, b->d_results, b->d_cursor, b->d_err};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (b->h_results) cudaFreeHost(b->h_results);
+  if (b->h_err) cudaFreeHost(b->h_err);
+  b->graph = nullptr;
+  b->d_arena = nullptr; b->d_circs = nullptr; b->d_tasks = nullptr; b->d_passes = nullptr;
+  b->d_stages = nullptr; b->d_ops = nullptr; b->d_obs = nullptr; b->d_counters = nullptr;
+  b->d_partials = nullptr; b->d_results = nullptr; b->d_cursor = nullptr; b->d_err = nullptr;
+  b->h_results = nullptr; b->h_err = nullptr;
+  b->built = false;
+}
+
+template <typename T>
+static cudaError_t upload(T** d, const std::vector<T>& h) {
+  const size_t bytes = std::max<size_t>(1, h.size()) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(d), bytes);
+  if (e != cudaSuccess) return e;
+  if (!h.empty()) e = cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+static cudaError_t batch_build(BatchImpl* b) {
+  batch_release(b);
+  if (!b->stream) {
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+  }
+  std::vector<BatchCirc> circs(b->entries.size());
+  std::vector<PassRec> passes;
+  std::vector<StageRec> stages;
+  std::vector<TileOp<float>> ops;
+  std::vector<double> obs;
+  uint64_t arena_amps = 0;
+  uint32_t counters = 0, partials = 0;
+  b->n_small = 0;
+  // per-circuit tiled plans, concatenated with rebased stage/op indices
+  for (size_t ci = 0; ci < b->entries.size(); ++ci) {
+    const BatchEntry& E = b->entries[ci];
+    BatchCirc& C = circs[ci];
+    std::memset(&C, 0, sizeof(C));
+    C.n = E.n;
+    C.small = E.n <= b->small_max ? 1 : 0;
+    TilePlan tp;
+    std::string err;
+    const int kmax = C.small ? 13 : std::min(b->plan_kmax, 13);
+    if (!build_tile_plan(lower_circuit(E.gates), E.n, DType::C64, kmax, &tp, &err)) return cudaErrorInvalidValue;
+    if (C.small && tp.passes.size() != 1) return cudaErrorInvalidValue;
+    C.pass_base = int32_t(passes.size());
+    C.n_passes = int32_t(tp.passes.size());
+    const int32_t sbase = int32_t(stages.size()), obase = int32_t(ops.size());
+    for (PassRec P : tp.passes) {
+      P.stage_begin += sbase;
+      P.stage_end += sbase;
+      passes.push_back(P);
+    }
+    for (StageRec S : tp.stages) {
+      S.op_begin += obase;
+      S.op_end += obase;
+      stages.push_back(S);
+    }
+    ops.insert(ops.end(), tp.ops_f.begin(), tp.ops_f.end());
+    C.obs_base = int32_t(obs.size());
+    obs.insert(obs.end(), E.J.begin(), E.J.end());
+    obs.insert(obs.end(), E.h.begin(), E.h.end());
+    C.result = int32_t(ci);
+    if (C.small) {
+      ++b->n_small;
+    } else {
+      C.amp_off = arena_amps;
+      arena_amps += 1ull << E.n;
+      C.done_base = int32_t(counters);
+      counters += uint32_t(C.n_passes) + 1;
+      C.meas_k = std::min(13, E.n);
+      C.meas_tiles = 1 << (E.n - C.meas_k);
+      C.part_base = int32_t(partials);
+      partials += uint32_t(C.meas_tiles);
+    }
+  }
+  b->n_passes_total = passes.size();
+  // task queue: every task depends only on tasks queued before it.
+  // Rounds r = 0, 1, ...: phase r of every large circuit (largest first; phase
+  // n_passes = measurement), all its tiles.  Small circuits are spread between
+  // rounds (order 0), placed first (order 1) or last (order 2).
+  std::vector<int> large, small;
+  for (size_t ci = 0; ci < circs.size(); ++ci) (circs[ci].small ? small : large).push_back(int(ci));
+  std::stable_sort(large.begin(), large.end(), [&](int a, int c) { return circs[a].n > circs[c].n; });
+  std::stable_sort(small.begin(), small.end(), [&](int a, int c) { return circs[a].n > circs[c].n; });
+  int max_rounds = 0;
+  for (int ci : large) max_rounds = std::max(max_rounds, circs[ci].n_passes + 1);
+  std::vector<BatchTask> tasks;
+  size_t si = 0;
+  auto push_small = [&](size_t upto) {
+    for (; si < std::min(upto, small.size()); ++si) tasks.push_back(BatchTask{small[si], -1, 0, 0});
+  };
+  if (b->order == 1) push_small(small.size());
+  for (int r = 0; r < max_rounds; ++r) {
+    for (int ci : large) {
+      const BatchCirc& C = circs[ci];
+      if (r > C.n_passes) continue;
+      const uint32_t tiles = r < C.n_passes ? (1u << passes[C.pass_base + r].n_out) : uint32_t(C.meas_tiles);
+      for (uint32_t t = 0; t < tiles; ++t) tasks.push_back(BatchTask{ci, r, t, 0});
+    }
+    if (b->order == 0) push_small(small.size() * size_t(r + 1) / size_t(max_rounds));
+  }
+  push_small(small.size());
+  b->n_tasks = uint32_t(tasks.size());
+  b->n_counters = std::max<uint32_t>(1, counters);
+  b->arena_bytes = size_t(arena_amps) * 8;
+
+  cudaError_t e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_arena), std::max<size_t>(16, b->arena_bytes))) != cudaSuccess) return e;
+  if ((e = upload(&b->d_circs, circs)) != cudaSuccess) return e;
+  if ((e = upload(&b->d_tasks, tasks)) != cudaSuccess) return e;
+  if ((e = upload(&b->d_passes, passes)) != cudaSuccess) return e;
+  if ((e = upload(&b->d_stages, stages)) != cudaSuccess) return e;
+  if ((e = upload(&b->d_ops, ops)) != cudaSuccess) return e;
+  if ((e = upload(&b->d_obs, obs)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_counters), sizeof(uint32_t) * b->n_counters)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_partials), sizeof(double) * std::max<uint32_t>(1, partials))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_results), sizeof(double) * std::max<size_t>(1, circs.size()))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_cursor), sizeof(uint32_t))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_err), sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(reinterpret_cast<void**>(&b->h_results), sizeof(double) * std::max<size_t>(1, circs.size()))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(reinterpret_cast<void**>(&b->h_err), sizeof(int))) != cudaSuccess) return e;
+
+  // capture: reset counters/cursor/error, the persistent launch, result copies
+  BatchLaunch L;
+  L.arena = b->d_arena; L.circs = b->d_circs; L.tasks = b->d_tasks; L.n_tasks = b->n_tasks;
+  L.passes = b->d_passes; L.stages = b->d_stages; L.ops = b->d_ops; L.obs = b->d_obs;
+  L.counters = b->d_counters; L.partials = b->d_partials; L.results = b->d_results;
+  L.cursor = b->d_cursor; L.err = b->d_err;
+  L.grid = unsigned(std::max(1, device_sms() * b->ctas_per_sm));
+  // warm the module and the smem attribute outside the capture
+  if ((e = cudaMemsetAsync(b->d_cursor, 0xFF, sizeof(uint32_t), b->stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream)) != cudaSuccess) return e;
+  BatchLaunch warm = L;
+  warm.n_tasks = 0;
+  warm.grid = 1;
+  if ((e = launch_batch(warm, b->stream)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return e;
+  cudaGraph_t g;
+  if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+  cudaMemsetAsync(b->d_counters, 0, sizeof(uint32_t) * b->n_counters, b->stream);
+  cudaMemsetAsync(b->d_cursor, 0, sizeof(uint32_t), b->stream);
+  cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream);
+  launch_batch(L, b->stream);
+  cudaMemcpyAsync(b->h_results, b->d_results, sizeof(double) * circs.size(), cudaMemcpyDeviceToHost, b->stream);
+  cudaMemcpyAsync(b->h_err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+  if ((e = cudaStreamEndCapture(b->stream, &g)) != cudaSuccess) return e;
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return e;
+  b->built = true;
+  return cudaSuccess;
+}
+
+}  // namespace nqpu
+
+using namespace nqpu;
+
+static BatchImpl* B(NqpuBatch* h) { return reinterpret_cast<BatchImpl*>(h); }
+
+extern "C" NqpuBatch* nqpu_batch_create(void) {
+  if (!device_ready()) return nullptr;
+  auto* b = new (std::nothrow) BatchImpl();
+  return reinterpret_cast<NqpuBatch*>(b);
+}
+
+extern "C" void nqpu_batch_destroy(NqpuBatch* batch) {
+  if (!batch) return;
+  BatchImpl* b = B(batch);
+  batch_release(b);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+extern "C" NqpuError nqpu_batch_add_ising(NqpuBatch* batch, const NqpuCircuit* circuit, const double* J,
+                                          const double* h, uint32_t* index) {
+  if (!batch || !circuit || !h) return NQPU_NULL_POINTER;
+  const CircuitImpl* c = reinterpret_cast<const CircuitImpl*>(circuit);
+  if (c->n < 5 || c->n > 24) return NQPU_INVALID_PARAMETER;  // batched circuits: 5..24 qubits (3 bond tables)
+  if (c->n > 1 && !J) return NQPU_NULL_POINTER;
+  BatchImpl* b = B(batch);
+  BatchEntry e;
+  e.n = int(c->n);
+  e.gates = c->gates;
+  e.J.assign(J, J + (c->n - 1));
+  e.h.assign(h, h + c->n);
+  if (index) *index = uint32_t(b->entries.size());
+  b->entries.push_back(std::move(e));
+  b->built = false;
+  return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_batch_config(NqpuBatch* batch, NqpuBatchParam param, int32_t value) {
+  if (!batch) return NQPU_NULL_POINTER;
+  BatchImpl* b = B(batch);
+  switch (param) {
+    case NQPU_BATCH_SMALL_MAX_QUBITS:
+      if (value < 5 || value > 13) return NQPU_INVALID_PARAMETER;
+      b->small_max = value;
+      break;
+    case NQPU_BATCH_TILE_QUBITS:
+      if (value < 10 || value > 13) return NQPU_INVALID_PARAMETER;
+      b->plan_kmax = value;
+      break;
+    case NQPU_BATCH_QUEUE_ORDER:
+      if (value < 0 || value > 2) return NQPU_INVALID_PARAMETER;
+      b->order = value;
+      break;
+    case NQPU_BATCH_CTAS_PER_SM:
+      if (value < 1 || value > 2) return NQPU_INVALID_PARAMETER;
+      b->ctas_per_sm = value;
+      break;
+    default:
+      return NQPU_INVALID_PARAMETER;
+  }
+  b->built = false;
+  return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_batch_prepare(NqpuBatch* batch) {
+  if (!batch) return NQPU_NULL_POINTER;
+  BatchImpl* b = B(batch);
+  if (b->entries.empty()) return NQPU_INVALID_PARAMETER;
+  const cudaError_t e = batch_build(b);
+  if (e == cudaErrorMemoryAllocation) return NQPU_ALLOCATION_FAILED;
+  if (e == cudaErrorInvalidValue) return NQPU_INVALID_PARAMETER;
+  return e == cudaSuccess ? NQPU_OK : NQPU_SIMULATION_FAILED;
+}
+
+extern "C" NqpuError nqpu_batch_run(NqpuBatch* batch, double* results, uint32_t len) {
+  if (!batch || !results) return NQPU_NULL_POINTER;
+  BatchImpl* b = B(batch);
+  if (len < b->entries.size()) return NQPU_INVALID_PARAMETER;
+  if (!b->built) {
+    NqpuError pe = nqpu_batch_prepare(batch);
+    if (pe != NQPU_OK) return pe;
+  }
+  if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return NQPU_SIMULATION_FAILED;
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return NQPU_SIMULATION_FAILED;
+  if (*b->h_err != 0) return NQPU_SIMULATION_FAILED;  // a bounded wait expired
+  std::memcpy(results, b->h_results, sizeof(double) * b->entries.size());
+  return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_batch_stats(const NqpuBatch* batch, uint64_t* out, uint32_t len) {
+  if (!batch || !out) return NQPU_NULL_POINTER;
+  if (len < 5) return NQPU_INVALID_PARAMETER;
+  const BatchImpl* b = reinterpret_cast<const BatchImpl*>(batch);
+  out[0] = b->entries.size();
+  out[1] = b->n_small;
+  out[2] = b->n_tasks;
+  out[3] = b->arena_bytes;
+  out[4] = b->n_passes_total;
+  return NQPU_OK;
+}

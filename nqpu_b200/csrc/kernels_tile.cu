@@ -17,415 +17,10 @@
 // Shared-memory layout: vector u (16 B) lives at slot swz(u) = u ^ fold3(u>>3)
 // so that the 8 lanes of a quarter-warp that the planner maps to vector bits of
 // distinct residue mod 3 hit 8 distinct 16-byte bank groups.
-#include "sv_device.cuh"
 #include "kernels.h"
+#include "tile_device.cuh"
 
 namespace nqpu {
-
-constexpr int kTileThreads = 256;
-constexpr int kVecPerThread = 16;
-
-__device__ __forceinline__ uint32_t swz(uint32_t u) {
-  uint32_t w = u >> 3;
-  uint32_t f = w ^ (w >> 3) ^ (w >> 6) ^ (w >> 9) ^ (w >> 12);
-  return u ^ (f & 7u);
-}
-
-template <typename C>
-__device__ __forceinline__ C csel(bool p, C a, C b) {
-  C r;
-  r.x = p ? a.x : b.x;
-  r.y = p ? a.y : b.y;
-  return r;
-}
-
-// ---- register-block op bodies (B, B0, B1, CB, ... are register-bit indices)
-// Every amplitude index i below is a compile-time constant after unrolling, so
-// the register block stays in registers; runtime register bits are turned into
-// template arguments by the dispatch switches.
-
-template <typename Real>
-__device__ __forceinline__ void ldc2(const Real* __restrict__ p, typename Tr<Real>::C& a,
-                                     typename Tr<Real>::C& b);
-template <>
-__device__ __forceinline__ void ldc2<float>(const float* __restrict__ p, float2& a, float2& b) {
-  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-  a = make_float2(v.x, v.y);
-  b = make_float2(v.z, v.w);
-}
-template <>
-__device__ __forceinline__ void ldc2<double>(const double* __restrict__ p, double2& a, double2& b) {
-  a = __ldg(reinterpret_cast<const double2*>(p));
-  b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-}
-
-// dense 2x2, no controls
-template <typename C, int NA, int B>
-__device__ __forceinline__ void rb_u1(C (&a)[NA], C m0, C m1, C m2, C m3) {
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    if (i & (1 << B)) continue;
-    const int j = i | (1 << B);
-    const C x = a[i], y = a[j];
-    a[i] = cmac2(m0, x, m1, y);
-    a[j] = cmac2(m2, x, m3, y);
-  }
-}
-
-// dense 2x2 with controls (generic: per-amplitude select)
-template <typename C, int NA, int B>
-__device__ __forceinline__ void rb_u1_ctrl(C (&a)[NA], C m0, C m1, C m2, C m3, bool tc, uint32_t creg) {
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    if (i & (1 << B)) continue;
-    const int j = i | (1 << B);
-    const bool cond = tc && ((uint32_t(i) & creg) == creg);
-    const C x = a[i], y = a[j];
-    a[i] = csel(cond, cmac2(m0, x, m1, y), x);
-    a[j] = csel(cond, cmac2(m2, x, m3, y), y);
-  }
-}
-
-template <typename C, int NA>
-__device__ __forceinline__ void rb_x1_generic(C (&a)[NA], int b, bool tc, uint32_t creg) {
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-#pragma unroll
-    for (int bb = 0; bb < 5; ++bb) {
-      if ((1 << bb) >= NA) break;
-      if (bb != b) continue;
-      if (i & (1 << bb)) continue;
-      const int j = i | (1 << bb);
-      const bool cond = tc && ((uint32_t(i) & creg) == creg);
-      const C x = a[i], y = a[j];
-      a[i] = csel(cond, y, x);
-      a[j] = csel(cond, x, y);
-    }
-  }
-}
-
-// phase m on the register amplitudes whose bits CMASK are all set
-template <typename C, int NA, int CMASK>
-__device__ __forceinline__ void rb_ph(C (&a)[NA], C m, bool neg) {
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    if ((i & CMASK) != CMASK) continue;
-    if (neg) {
-      a[i].x = -a[i].x;
-      a[i].y = -a[i].y;
-    } else {
-      a[i] = cmul(m, a[i]);
-    }
-  }
-}
-
-// diag(d0, d1) selected by register bit DB (DB == NA_BITS: the thread-level bit tb)
-template <typename C, int NA, int DB, int NRB>
-__device__ __forceinline__ void rb_d1(C (&a)[NA], C d0, C d1, uint32_t tb) {
-  if constexpr (DB >= NRB) {
-    const C d = csel(tb != 0, d1, d0);
-#pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul(d, a[i]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul((i & (1 << DB)) ? d1 : d0, a[i]);
-  }
-}
-
-// diag on two bits (register bit or thread-level bit when >= NRB)
-template <typename C, int NA, int D0, int D1, int NRB>
-__device__ __forceinline__ void rb_d2(C (&a)[NA], const C* m, uint32_t tb0, uint32_t tb1) {
-  if constexpr (D0 >= NRB && D1 >= NRB) {
-    const C lo = csel(tb0 != 0, m[1], m[0]);
-    const C hi = csel(tb0 != 0, m[3], m[2]);
-    const C d = csel(tb1 != 0, hi, lo);
-#pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul(d, a[i]);
-  } else if constexpr (D0 >= NRB) {
-    const C lo = csel(tb0 != 0, m[1], m[0]);
-    const C hi = csel(tb0 != 0, m[3], m[2]);
-#pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul((i & (1 << D1)) ? hi : lo, a[i]);
-  } else if constexpr (D1 >= NRB) {
-    const C lo = csel(tb1 != 0, m[2], m[0]);
-    const C hi = csel(tb1 != 0, m[3], m[1]);
-#pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul((i & (1 << D0)) ? hi : lo, a[i]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < NA; ++i) {
-      const int k = ((i >> D0) & 1) | (((i >> D1) & 1) << 1);
-      a[i] = cmul(m[k], a[i]);
-    }
-  }
-}
-
-// generic diagonal with controls: d selected per amplitude at run time
-template <typename C, int NA>
-__device__ __forceinline__ void rb_diag_generic(C (&a)[NA], const C* m, int nd, uint32_t dreg0,
-                                                uint32_t dreg1, uint32_t tb0, uint32_t tb1, bool tc,
-                                                uint32_t creg) {
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    const bool cond = tc && ((uint32_t(i) & creg) == creg);
-    const uint32_t b0 = (dreg0 != 0xFF) ? ((uint32_t(i) >> dreg0) & 1u) : tb0;
-    const uint32_t b1 = (nd > 1) ? ((dreg1 != 0xFF) ? ((uint32_t(i) >> dreg1) & 1u) : tb1) : 0u;
-    const C lo = csel(b0 != 0, m[1], m[0]);
-    const C hi = csel(b0 != 0, m[3], m[2]);
-    const C d = csel(b1 != 0, hi, lo);
-    a[i] = csel(cond, cmul(d, a[i]), a[i]);
-  }
-}
-
-// dense 4x4 on register bits (B0 = sub-index bit 0, B1 = bit 1); matrix rows
-// are read from the op record (L1-resident) per quad to keep registers free.
-template <typename Real, typename C, int NA, int B0, int B1>
-__device__ __forceinline__ void rb_u2(C (&a)[NA], const Real* __restrict__ mp, bool tc, uint32_t creg) {
-  constexpr int M0 = 1 << B0, M1 = 1 << B1;
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    if (i & (M0 | M1)) continue;
-    const bool cond = tc && ((uint32_t(i) & creg) == creg);
-    const C x0 = a[i], x1 = a[i | M0], x2 = a[i | M1], x3 = a[i | M0 | M1];
-    C y[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      C m[4];
-      ldc2<Real>(mp + 8 * r, m[0], m[1]);
-      ldc2<Real>(mp + 8 * r + 4, m[2], m[3]);
-      y[r] = cmac4(m, x0, x1, x2, x3);
-    }
-    a[i] = csel(cond, y[0], x0);
-    a[i | M0] = csel(cond, y[1], x1);
-    a[i | M1] = csel(cond, y[2], x2);
-    a[i | M0 | M1] = csel(cond, y[3], x3);
-  }
-}
-
-template <typename C, int NA, int B0, int B1>
-__device__ __forceinline__ void rb_sw(C (&a)[NA], bool tc, uint32_t creg) {
-  constexpr int M0 = 1 << B0, M1 = 1 << B1;
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    if (i & (M0 | M1)) continue;
-    const bool cond = tc && ((uint32_t(i) & creg) == creg);
-    const C x1 = a[i | M0], x2 = a[i | M1];
-    a[i | M0] = csel(cond, x2, x1);
-    a[i | M1] = csel(cond, x1, x2);
-  }
-}
-
-// ---- dispatch helpers ------------------------------------------------------
-#define NQ_REG_CASES(M, ...) M(0, __VA_ARGS__) M(1, __VA_ARGS__) M(2, __VA_ARGS__) M(3, __VA_ARGS__) M(4, __VA_ARGS__)
-
-template <typename C, int NA, int NRB>
-__device__ __forceinline__ void dispatch_ph(C (&a)[NA], uint32_t creg, C m, bool neg) {
-  switch (creg) {
-#define NQ_PHC(V) case V: if constexpr (V < (1 << NRB)) rb_ph<C, NA, V>(a, m, neg); break;
-    NQ_PHC(0) NQ_PHC(1) NQ_PHC(2) NQ_PHC(3) NQ_PHC(4) NQ_PHC(5) NQ_PHC(6) NQ_PHC(7)
-    NQ_PHC(8) NQ_PHC(9) NQ_PHC(10) NQ_PHC(11) NQ_PHC(12) NQ_PHC(13) NQ_PHC(14) NQ_PHC(15)
-    NQ_PHC(16) NQ_PHC(17) NQ_PHC(18) NQ_PHC(19) NQ_PHC(20) NQ_PHC(21) NQ_PHC(22) NQ_PHC(23)
-    NQ_PHC(24) NQ_PHC(25) NQ_PHC(26) NQ_PHC(27) NQ_PHC(28) NQ_PHC(29) NQ_PHC(30) NQ_PHC(31)
-#undef NQ_PHC
-    default: break;
-  }
-}
-
-template <typename C, int NA, int NRB, int D0>
-__device__ __forceinline__ void dispatch_d2_b(C (&a)[NA], int d1, const C* m, uint32_t tb0, uint32_t tb1) {
-  switch (d1) {
-#define NQ_D2B(V) case V: if constexpr (V <= NRB && (V != D0 || V == NRB)) rb_d2<C, NA, D0, V, NRB>(a, m, tb0, tb1); break;
-    NQ_D2B(0) NQ_D2B(1) NQ_D2B(2) NQ_D2B(3) NQ_D2B(4) NQ_D2B(5)
-#undef NQ_D2B
-    default: break;
-  }
-}
-
-template <typename Real, typename C, int NA, int NRB, int B0>
-__device__ __forceinline__ void dispatch_u2_b(C (&a)[NA], int b1, const Real* mp, bool tc, uint32_t creg) {
-  switch (b1) {
-#define NQ_U2B(V) case V: if constexpr (V < NRB && V != B0) rb_u2<Real, C, NA, B0, V>(a, mp, tc, creg); break;
-    NQ_U2B(0) NQ_U2B(1) NQ_U2B(2) NQ_U2B(3) NQ_U2B(4)
-#undef NQ_U2B
-    default: break;
-  }
-}
-
-template <typename C, int NA, int NRB, int B0>
-__device__ __forceinline__ void dispatch_sw_b(C (&a)[NA], int b1, bool tc, uint32_t creg) {
-  switch (b1) {
-#define NQ_SWB(V) case V: if constexpr (V < NRB && V != B0) rb_sw<C, NA, B0, V>(a, tc, creg); break;
-    NQ_SWB(0) NQ_SWB(1) NQ_SWB(2) NQ_SWB(3) NQ_SWB(4)
-#undef NQ_SWB
-    default: break;
-  }
-}
-
-// Apply ops [ob, oe) of a stage to the thread's register block.
-// vbase = virtual index of register amplitude 0 (register bits are zero in it).
-template <typename Real, int NA, int NRB>
-__device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
-                                                const TileOp<Real>* __restrict__ ops, int ob,
-                                                int oe, uint32_t vbase) {
-  using C = typename Tr<Real>::C;
-  for (int o = ob; o < oe; ++o) {
-    const TileOp<Real>* op = ops + o;
-    const uint4 h0 = __ldg(reinterpret_cast<const uint4*>(op));
-    const uint32_t dv1 = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
-    const uint32_t kind = h0.x & 0xFF;
-    const uint32_t rb0 = (h0.x >> 8) & 0xFF;
-    const uint32_t rb1 = (h0.x >> 16) & 0xFF;
-    const uint32_t creg = (h0.x >> 24) & 0xFF;
-    const uint32_t dreg0 = h0.y & 0xFF;
-    const uint32_t dreg1 = (h0.y >> 8) & 0xFF;
-    const uint32_t cnr = h0.z;
-    const uint32_t dv0 = h0.w;
-    const bool tc = (vbase & cnr) == cnr;
-    const Real* mp = op->m;
-    switch (kind) {
-      case OP_U1: {
-        C m0, m1, m2, m3;
-        ldc2<Real>(mp, m0, m1);
-        ldc2<Real>(mp + 4, m2, m3);
-        if (creg == 0) {
-          if (!tc) break;
-          switch (rb0) {
-#define NQ_U1(B, _) case B: if constexpr (B < NRB) rb_u1<C, NA, B>(a, m0, m1, m2, m3); break;
-            NQ_REG_CASES(NQ_U1, 0)
-#undef NQ_U1
-            default: break;
-          }
-        } else {
-          switch (rb0) {
-#define NQ_U1C(B, _) case B: if constexpr (B < NRB) rb_u1_ctrl<C, NA, B>(a, m0, m1, m2, m3, tc, creg); break;
-            NQ_REG_CASES(NQ_U1C, 0)
-#undef NQ_U1C
-            default: break;
-          }
-        }
-        break;
-      }
-      case OP_X1: {
-        // Only X1 ops the planner could not defer into the stage's write-back
-        // permutation reach the kernel (e.g. Toffoli).  They use selects, not
-        // register swaps: a register permutation at this join would make the
-        // allocator insert moves into every other op's path.
-        rb_x1_generic<C, NA>(a, int(rb0), tc, creg);
-        break;
-      }
-      case OP_PH: {
-        if (!tc) break;
-        C m0, m1;
-        ldc2<Real>(mp, m0, m1);
-        const bool neg = (m0.x == Real(-1)) && (m0.y == Real(0));
-        dispatch_ph<C, NA, NRB>(a, creg, m0, neg);
-        break;
-      }
-      case OP_D1: {
-        C m[4];
-        ldc2<Real>(mp, m[0], m[1]);
-        const uint32_t tb = (vbase & dv0) ? 1u : 0u;
-        if (creg == 0 && cnr == 0) {
-          switch (dreg0 == 0xFF ? NRB : int(dreg0)) {
-#define NQ_D1(B, _) case B: if constexpr (B <= NRB) rb_d1<C, NA, B, NRB>(a, m[0], m[1], tb); break;
-            NQ_REG_CASES(NQ_D1, 0)
-            case 5: if constexpr (NRB == 5) rb_d1<C, NA, 5, NRB>(a, m[0], m[1], tb); break;
-#undef NQ_D1
-            default: break;
-          }
-        } else {
-          m[2] = m[0];
-          m[3] = m[1];
-          rb_diag_generic<C, NA>(a, m, 1, dreg0, 0xFF, tb, 0, tc, creg);
-        }
-        break;
-      }
-      case OP_D2: {
-        C m[4];
-        ldc2<Real>(mp, m[0], m[1]);
-        ldc2<Real>(mp + 4, m[2], m[3]);
-        const uint32_t tb0 = (vbase & dv0) ? 1u : 0u;
-        const uint32_t tb1 = (vbase & dv1) ? 1u : 0u;
-        if (creg == 0 && cnr == 0) {
-          const int d0 = dreg0 == 0xFF ? NRB : int(dreg0);
-          const int d1 = dreg1 == 0xFF ? NRB : int(dreg1);
-          switch (d0) {
-#define NQ_D2A(V) case V: if constexpr (V <= NRB) dispatch_d2_b<C, NA, NRB, V>(a, d1, m, tb0, tb1); break;
-            NQ_D2A(0) NQ_D2A(1) NQ_D2A(2) NQ_D2A(3) NQ_D2A(4) NQ_D2A(5)
-#undef NQ_D2A
-            default: break;
-          }
-        } else {
-          rb_diag_generic<C, NA>(a, m, 2, dreg0, dreg1, tb0, tb1, tc, creg);
-        }
-        break;
-      }
-      case OP_U2: {
-        switch (rb0) {
-#define NQ_U2A(B, _) case B: if constexpr (B < NRB) dispatch_u2_b<Real, C, NA, NRB, B>(a, rb1, mp, tc, creg); break;
-          NQ_REG_CASES(NQ_U2A, 0)
-#undef NQ_U2A
-          default: break;
-        }
-        break;
-      }
-      case OP_SW: {
-        switch (rb0) {
-#define NQ_SWA(B, _) case B: if constexpr (B < NRB) dispatch_sw_b<C, NA, NRB, B>(a, rb1, tc, creg); break;
-          NQ_REG_CASES(NQ_SWA, 0)
-#undef NQ_SWA
-          default: break;
-        }
-        break;
-      }
-      default:
-        break;
-    }
-  }
-}
-
-template <typename Real>
-__device__ __forceinline__ void unpack_vec(const typename Tr<Real>::V& v, typename Tr<Real>::C* a);
-template <>
-__device__ __forceinline__ void unpack_vec<float>(const float4& v, float2* a) {
-  a[0] = make_float2(v.x, v.y);
-  a[1] = make_float2(v.z, v.w);
-}
-template <>
-__device__ __forceinline__ void unpack_vec<double>(const double2& v, double2* a) {
-  a[0] = v;
-}
-template <typename Real>
-__device__ __forceinline__ typename Tr<Real>::V pack_vec(const typename Tr<Real>::C* a);
-template <>
-__device__ __forceinline__ float4 pack_vec<float>(const float2* a) {
-  return make_float4(a[0].x, a[0].y, a[1].x, a[1].y);
-}
-template <>
-__device__ __forceinline__ double2 pack_vec<double>(const double2* a) {
-  return a[0];
-}
-template <typename Real>
-__device__ __forceinline__ typename Tr<Real>::V pack_vec(typename Tr<Real>::C lo, typename Tr<Real>::C hi) {
-  typename Tr<Real>::C t[2] = {lo, hi};
-  return pack_vec<Real>(t);
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// Global amplitude index of tile-local index 0 of `tile` (tile id bit j -> qout[j]).
-__device__ __forceinline__ uint64_t tile_base(const PassRec& P, uint64_t tile) {
-  uint64_t base = 0;
-  for (int j = 0; j < P.n_out; ++j)
-    if ((tile >> j) & 1ull) base |= 1ull << P.qout[j];
-  return base;
-}
 
 // Dynamic shared memory: [tile buffer 0 | tile buffer 1 | hi_off table (2^(k-c) u64)].
 // One persistent CTA per SM: while the stages of tile i run on one buffer, the
@@ -436,12 +31,8 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
                 const StageRec* __restrict__ stages, const TileOp<Real>* __restrict__ ops,
                 int pass_idx, uint64_t n_tiles) {
   using T = Tr<Real>;
-  using C = typename T::C;
   using V = typename T::V;
   constexpr int VB = T::kVecBit;
-  constexpr int APV = T::kAmpsPerVec;
-  constexpr int NA = kVecPerThread * APV;  // amplitudes per thread
-  constexpr int NRB = VB + kRegFree;       // register bits
   constexpr uint32_t kMaxVec = 1u << (KMAX - VB);
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -469,7 +60,6 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
   }
   __syncthreads();
   const uint32_t lowmask = (1u << c) - 1u;
-  const uint32_t active_threads = nvec / kVecPerThread;
 
   // HBM -> shared, asynchronous (consecutive threads take consecutive vectors).
   auto issue_load = [&](uint64_t tile, V* dst) {
@@ -508,89 +98,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     for (int j = 0; j < P.n_ext; ++j)
       if ((base >> P.ext[j]) & 1ull) ext |= 1u << (k + j);
 
-    for (int s = P.stage_begin; s < P.stage_end; ++s) {
-      const StageRec* S = stages + s;
-      if (uint32_t(tid) < active_threads) {
-        const int ntb = __ldg(&S->n_tbits);
-        uint32_t ub = 0;
-        for (int j = 0; j < ntb; ++j) ub |= ((uint32_t(tid) >> j) & 1u) << __ldg(&S->tpos[j]);
-        // swz is linear over XOR and ub, vm_i have disjoint bits, so
-        // swz(ub | sum vm_i) = swz(ub) ^ xor_i swz(vm_i).
-        const uint32_t s0 = swz(1u << (__ldg(&S->rpos[0]) - VB));
-        const uint32_t s1 = swz(1u << (__ldg(&S->rpos[1]) - VB));
-        const uint32_t s2 = swz(1u << (__ldg(&S->rpos[2]) - VB));
-        const uint32_t s3 = swz(1u << (__ldg(&S->rpos[3]) - VB));
-        const uint32_t sb = swz(ub);
-        C a[NA];
-#pragma unroll
-        for (int r = 0; r < kVecPerThread; ++r) {
-          const uint32_t slot = sb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
-                                ((r & 4) ? s2 : 0u) ^ ((r & 8) ? s3 : 0u);
-          unpack_vec<Real>(sv[slot], a + r * APV);
-        }
-        const uint32_t vbase = (ub << VB) | ext;
-        apply_stage_ops<Real, NA, NRB>(a, ops, __ldg(&S->op_begin), __ldg(&S->op_end), vbase);
-        // Write-back through the stage's deferred permutation pi(p) = A p ^ w:
-        // register amplitude p goes to the slot of logical index pi(p).  Slot
-        // offsets are linear in the free register bits (register bits
-        // VB..VB+3); for complex64, bit 0 of pi(p) selects the 8-byte half.
-        auto regslot = [&](uint32_t m) -> uint32_t {
-          return (((m >> VB) & 1u) ? s0 : 0u) ^ (((m >> (VB + 1)) & 1u) ? s1 : 0u) ^
-                 (((m >> (VB + 2)) & 1u) ? s2 : 0u) ^ (((m >> (VB + 3)) & 1u) ? s3 : 0u);
-        };
-        uint32_t w = uint32_t(__ldg(&S->sbx));
-        const int nc = __ldg(&S->ncond);
-        for (int i = 0; i < nc; ++i) {
-          const uint32_t cm = __ldg(&S->cond_cnr[i]);
-          if ((vbase & cm) == cm) w ^= uint32_t(__ldg(&S->cond_w[i]));
-        }
-        const uint32_t m0 = uint32_t(__ldg(&S->scol[VB]));
-        const uint32_t m1 = uint32_t(__ldg(&S->scol[VB + 1]));
-        const uint32_t m2 = uint32_t(__ldg(&S->scol[VB + 2]));
-        const uint32_t m3 = uint32_t(__ldg(&S->scol[VB + 3]));
-        const uint32_t c0 = regslot(m0), c1 = regslot(m1), c2 = regslot(m2), c3 = regslot(m3);
-        const uint32_t sw = sb ^ regslot(w);
-        if constexpr (VB == 1) {
-          const uint32_t mz = uint32_t(__ldg(&S->scol[0]));
-          if (mz == 1u) {
-            // bit 0 stays bit 0: each vector keeps its pair, halves swap when
-            // bit 0 of pi is flipped by the other register bits or by w
-            const uint32_t h0 = m0 & 1u, h1 = m1 & 1u, h2 = m2 & 1u, h3 = m3 & 1u, hw = w & 1u;
-#pragma unroll
-            for (int r = 0; r < kVecPerThread; ++r) {
-              const uint32_t slot = sw ^ ((r & 1) ? c0 : 0u) ^ ((r & 2) ? c1 : 0u) ^
-                                    ((r & 4) ? c2 : 0u) ^ ((r & 8) ? c3 : 0u);
-              const uint32_t hs = hw ^ ((r & 1) ? h0 : 0u) ^ ((r & 2) ? h1 : 0u) ^
-                                  ((r & 4) ? h2 : 0u) ^ ((r & 8) ? h3 : 0u);
-              const C lo = a[2 * r], hi = a[2 * r + 1];
-              sv[slot] = hs ? pack_vec<Real>(hi, lo) : pack_vec<Real>(lo, hi);
-            }
-          } else {
-            // bit 0 moves into other bits: store each amplitude separately
-            const uint32_t cz = regslot(mz), hz = mz & 1u;
-            const uint32_t h0 = m0 & 1u, h1 = m1 & 1u, h2 = m2 & 1u, h3 = m3 & 1u, hw = w & 1u;
-            C* sa = reinterpret_cast<C*>(sv);
-#pragma unroll
-            for (int r = 0; r < kVecPerThread; ++r) {
-              const uint32_t slot = sw ^ ((r & 1) ? c0 : 0u) ^ ((r & 2) ? c1 : 0u) ^
-                                    ((r & 4) ? c2 : 0u) ^ ((r & 8) ? c3 : 0u);
-              const uint32_t hs = hw ^ ((r & 1) ? h0 : 0u) ^ ((r & 2) ? h1 : 0u) ^
-                                  ((r & 4) ? h2 : 0u) ^ ((r & 8) ? h3 : 0u);
-              sa[2 * slot + hs] = a[2 * r];
-              sa[2 * (slot ^ cz) + (hs ^ hz)] = a[2 * r + 1];
-            }
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < kVecPerThread; ++r) {
-            const uint32_t slot = sw ^ ((r & 1) ? c0 : 0u) ^ ((r & 2) ? c1 : 0u) ^
-                                  ((r & 4) ? c2 : 0u) ^ ((r & 8) ? c3 : 0u);
-            sv[slot] = pack_vec<Real>(a + r * APV);
-          }
-        }
-      }
-      __syncthreads();
-    }
+    run_tile_stages<Real>(sv, P, stages, ops, ext);
 
     // shared -> HBM
 #pragma unroll
