@@ -296,8 +296,12 @@ NqpuError   nqpu_batch_config(NqpuBatch* batch, NqpuBatchParam param, int32_t va
 NqpuError   nqpu_batch_prepare(NqpuBatch* batch);
 /* Replay the graph; results[i] = <H> of circuit i (FP64).  len >= circuits. */
 NqpuError   nqpu_batch_run(NqpuBatch* batch, double* results, uint32_t len);
-/* out[0..4] = circuits, small circuits, tasks, HBM arena bytes, tiled passes. */
+/* out[0..4] = circuits, small circuits, tasks, HBM arena bytes, tiled passes;
+ * out[5] (len >= 6) = bytes of tables uploaded host->device by prepare(). */
 NqpuError   nqpu_batch_stats(const NqpuBatch* batch, uint64_t* out, uint32_t len);
+/* Device time of the last run() (CUDA events around the graph replay on the
+ * batch's stream: counter resets, the persistent launch, the result copy). */
+NqpuError   nqpu_batch_last_run_ms(const NqpuBatch* batch, float* ms);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -54,10 +54,17 @@ class Batch:
         check(self.lib.nqpu_batch_run(self.h_, out.ctypes.data_as(C.POINTER(C.c_double)), self.count), "batch_run")
         return out
 
+    def last_run_ms(self) -> float:
+        """Device time of the last run() (CUDA events around the graph replay)."""
+        ms = C.c_float()
+        check(self.lib.nqpu_batch_last_run_ms(self.h_, C.byref(ms)), "batch_last_run_ms")
+        return float(ms.value)
+
     def stats(self) -> dict:
-        out = (C.c_uint64 * 5)()
-        check(self.lib.nqpu_batch_stats(self.h_, out, 5), "batch_stats")
-        return {"circuits": out[0], "small": out[1], "tasks": out[2], "arena_bytes": out[3], "passes": out[4]}
+        out = (C.c_uint64 * 6)()
+        check(self.lib.nqpu_batch_stats(self.h_, out, 6), "batch_stats")
+        return {"circuits": out[0], "small": out[1], "tasks": out[2], "arena_bytes": out[3], "passes": out[4],
+                "upload_bytes": out[5]}
 
 
 def ising_terms(n, J, h):

@@ -45,8 +45,10 @@ struct BatchImpl {
   double* h_results = nullptr;
   int* h_err = nullptr;
   uint32_t n_tasks = 0, n_counters = 0;
-  size_t arena_bytes = 0, n_small = 0, n_passes_total = 0;
+  size_t arena_bytes = 0, n_small = 0, n_passes_total = 0, upload_bytes = 0;
   cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;  // bracket each graph replay on `stream`
+  bool timed = false;
 };
 
 static void batch_release(BatchImpl* b) {
@@ -171,6 +173,9 @@ static cudaError_t batch_build(BatchImpl* b) {
   if ((e = upload(&b->d_stages, stages)) != cudaSuccess) return e;
   if ((e = upload(&b->d_ops, ops)) != cudaSuccess) return e;
   if ((e = upload(&b->d_obs, obs)) != cudaSuccess) return e;
+  b->upload_bytes = circs.size() * sizeof(BatchCirc) + tasks.size() * sizeof(BatchTask) +
+                    passes.size() * sizeof(PassRec) + stages.size() * sizeof(StageRec) +
+                    ops.size() * sizeof(TileOp<float>) + obs.size() * sizeof(double);
   if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_counters), sizeof(uint32_t) * b->n_counters)) != cudaSuccess) return e;
   if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_partials), sizeof(double) * std::max<uint32_t>(1, partials))) != cudaSuccess) return e;
   if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_results), sizeof(double) * std::max<size_t>(1, circs.size()))) != cudaSuccess) return e;
@@ -226,6 +231,8 @@ extern "C" void nqpu_batch_destroy(NqpuBatch* batch) {
   if (!batch) return;
   BatchImpl* b = B(batch);
   batch_release(b);
+  if (b->ev_begin) cudaEventDestroy(b->ev_begin);
+  if (b->ev_end) cudaEventDestroy(b->ev_end);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -293,8 +300,13 @@ extern "C" NqpuError nqpu_batch_run(NqpuBatch* batch, double* results, uint32_t 
     NqpuError pe = nqpu_batch_prepare(batch);
     if (pe != NQPU_OK) return pe;
   }
+  if (!b->ev_begin && (cudaEventCreate(&b->ev_begin) != cudaSuccess || cudaEventCreate(&b->ev_end) != cudaSuccess))
+    return NQPU_SIMULATION_FAILED;
+  if (cudaEventRecord(b->ev_begin, b->stream) != cudaSuccess) return NQPU_SIMULATION_FAILED;
   if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return NQPU_SIMULATION_FAILED;
+  if (cudaEventRecord(b->ev_end, b->stream) != cudaSuccess) return NQPU_SIMULATION_FAILED;
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return NQPU_SIMULATION_FAILED;
+  b->timed = true;
   if (*b->h_err != 0) return NQPU_SIMULATION_FAILED;  // a bounded wait expired
   std::memcpy(results, b->h_results, sizeof(double) * b->entries.size());
   return NQPU_OK;
@@ -309,5 +321,13 @@ extern "C" NqpuError nqpu_batch_stats(const NqpuBatch* batch, uint64_t* out, uin
   out[2] = b->n_tasks;
   out[3] = b->arena_bytes;
   out[4] = b->n_passes_total;
+  if (len >= 6) out[5] = b->upload_bytes;
   return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_batch_last_run_ms(const NqpuBatch* batch, float* ms) {
+  if (!batch || !ms) return NQPU_NULL_POINTER;
+  const BatchImpl* b = reinterpret_cast<const BatchImpl*>(batch);
+  if (!b->timed) return NQPU_INVALID_PARAMETER;
+  return cudaEventElapsedTime(ms, b->ev_begin, b->ev_end) == cudaSuccess ? NQPU_OK : NQPU_SIMULATION_FAILED;
 }
