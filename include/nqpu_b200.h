@@ -303,6 +303,51 @@ NqpuError   nqpu_batch_stats(const NqpuBatch* batch, uint64_t* out, uint32_t len
  * batch's stream: counter resets, the persistent launch, the result copy). */
 NqpuError   nqpu_batch_last_run_ms(const NqpuBatch* batch, float* ms);
 
+/* ------------------------------------------------------------------ */
+/* Serving (no counterpart in the reference): a request loop that runs  */
+/* circuits of mixed sizes on device-resident complex64 states.         */
+/* Requests are admitted while others run, as lanes (CUDA streams) and  */
+/* HBM budget (2^n x 8 B per state, buddy-allocated in one arena) free  */
+/* up, so their kernels overlap on the GPU.  Every handle call is       */
+/* thread-safe; results are the same whether a request runs alone or    */
+/* in a mix.                                                            */
+/* ------------------------------------------------------------------ */
+typedef struct NqpuServer NqpuServer;
+typedef enum {
+    NQPU_REQUEST_ZALL  = 0,  /* all <Z_i> (FP64) */
+    NQPU_REQUEST_SHOTS = 1   /* `shots` samples drawn with the request's seed (xorshift64*, as nqpu_set_seed) */
+} NqpuRequestKind;
+typedef struct {
+    uint64_t hbm_budget_bytes; /* resident-state budget; 0 = half of the free device memory */
+    uint32_t max_qubits;       /* largest request (<= 32; 0 = 28) */
+    uint32_t lanes;            /* requests on the device at once (0 = 16) */
+    uint32_t large_lanes;      /* of which large requests may hold (0 = 2) */
+    uint32_t large_qubits;     /* "large" = at least this many qubits (0 = 22) */
+    uint32_t max_shots;        /* largest shot request (0 = 1024) */
+} NqpuServerConfig;
+
+/* NULL on no device, bad config, or a budget below one largest state. */
+NqpuServer* nqpu_server_create(const NqpuServerConfig* config);
+/* Drops queued requests, waits for running ones, frees everything. */
+void        nqpu_server_destroy(NqpuServer* server);
+/* Plans the circuit (copied; the handle may be destroyed afterwards) and
+ * queues it; *request_id > 0. */
+NqpuError   nqpu_server_submit(NqpuServer* server, const NqpuCircuit* circuit, NqpuRequestKind kind,
+                               uint32_t shots, uint64_t seed, uint64_t* request_id);
+/* *done = 1 once the request finished (non-blocking). */
+NqpuError   nqpu_server_poll(NqpuServer* server, uint64_t request_id, int32_t* done);
+/* Block until the request (request_id = 0: every submitted request) finished;
+ * NQPU_SIMULATION_FAILED after timeout_s (<= 0: one hour). */
+NqpuError   nqpu_server_wait(NqpuServer* server, uint64_t request_id, double timeout_s);
+/* Copy a finished request's result and release it: out_z[0..n) for ZALL,
+ * out_shots[0..shots) for SHOTS; timing_ms (optional, 3 values) = queued,
+ * running, total milliseconds from submit to completion. */
+NqpuError   nqpu_server_result(NqpuServer* server, uint64_t request_id, double* out_z, uint32_t z_len,
+                               uint64_t* out_shots, uint32_t shots_len, double* timing_ms);
+/* out[0..7] = submitted, completed, failed, running, queued, peak resident
+ * bytes, arena bytes, peak concurrent requests.  len >= 8. */
+NqpuError   nqpu_server_stats(NqpuServer* server, uint64_t* out, uint32_t len);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -28,6 +28,11 @@ class NqpuVersion(C.Structure):
     _fields_ = [("major", C.c_uint32), ("minor", C.c_uint32), ("patch", C.c_uint32)]
 
 
+class NqpuServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_qubits", C.c_uint32), ("lanes", C.c_uint32),
+                ("large_lanes", C.c_uint32), ("large_qubits", C.c_uint32), ("max_shots", C.c_uint32)]
+
+
 _SCALARS = {
     "void": None,
     "bool": C.c_bool,
@@ -40,6 +45,8 @@ _SCALARS = {
     "NqpuDtype": C.c_int,
     "NqpuMode": C.c_int,
     "NqpuBatchParam": C.c_int,
+    "NqpuRequestKind": C.c_int,
+    "NqpuServerConfig": NqpuServerConfig,
     "int32_t": C.c_int32,
     "NqpuComplex": NqpuComplex,
     "NqpuVersion": NqpuVersion,

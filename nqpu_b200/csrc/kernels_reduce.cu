@@ -46,7 +46,7 @@ __device__ __forceinline__ void vec_probs<double>(const double2& v, double* p) {
 
 // Layout of the zsums scratch (doubles):
 //   [0, nblk*kBlkVals)            per-block low-bit partials
-//   [zs_seg_off, + nseg*8)        per-warp segment partials
+//   [kZsMaxBlocks*kBlkVals, + nseg) per-segment totals (room is kept for 8 per segment)
 constexpr int kBlkVals = 16;  // tot, bit0(c64), 8 thread bits, 4 j bits, (pad)
 constexpr int kZsMaxBlocks = 1024;
 
@@ -62,6 +62,8 @@ __global__ void __launch_bounds__(kRedThreads)
   KSum tot, b0;
   KSum jb[4];
   const V* vp = reinterpret_cast<const V*>(amp);
+  static_assert(kRedThreads == 256, "segment total sums 8 warps");
+  __shared__ double seg_red[kRedThreads / 32];
   for (uint64_t seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
     const uint64_t vbase = seg * (kRedThreads * kRedVecPerThread);
     V v[kRedVecPerThread];
@@ -90,7 +92,12 @@ __global__ void __launch_bounds__(kRedThreads)
       }
     }
     segp = warp_sum(segp);
-    if (lane == 0) seg_part[seg * 8 + warp] = segp;
+    if (lane == 0) seg_red[warp] = segp;
+    __syncthreads();
+    if (tid == 0)
+      seg_part[seg] = ((seg_red[0] + seg_red[1]) + (seg_red[2] + seg_red[3])) +
+                      ((seg_red[4] + seg_red[5]) + (seg_red[6] + seg_red[7]));
+    __syncthreads();
   }
   // Per-block partials of the low bits: thread bits come from the per-thread totals.
   __shared__ double red[kRedThreads / 32][kBlkVals];
@@ -120,7 +127,7 @@ __global__ void __launch_bounds__(kRedThreads)
 template <int VB>
 __global__ void __launch_bounds__(1024)
     k_zsums_final(int n, int nblk, uint64_t nseg, int H, const double* __restrict__ blk_part,
-                  const double* __restrict__ seg_part, double* __restrict__ out) {
+                  double* __restrict__ seg_part, double* __restrict__ out) {
   __shared__ double sh[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   auto block_sum = [&](double v) -> double {
@@ -152,17 +159,22 @@ __global__ void __launch_bounds__(1024)
       else if (qbit >= 0 && qbit < n && qbit < H) out[1 + qbit] = s;
     }
   }
-  for (int q = H; q < n; ++q) {
-    const int b = q - H;
+  // High bits: nseg is a power of two (2^(n-H)).  Fold the segment totals in
+  // half, top bit first: at level b the upper half A[2^b .. 2^(b+1)) sums to the
+  // weight of amplitude bit H + b, and A[i] += A[i + 2^b] leaves A[0 .. 2^b)
+  // indexed by the lower segment bits.  In place: at each level every i is
+  // read and written by one thread only; block_sum's barriers order the levels.
+  double* A = seg_part;
+  for (int b = n - H - 1; b >= 0; --b) {
+    const uint64_t half = 1ull << b;
     KSum acc;
-    for (uint64_t sgi = tid; sgi < nseg; sgi += blockDim.x) {
-      if ((sgi >> b) & 1ull) {
-        const double* p = seg_part + sgi * 8;
-        acc.add(((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7])));
-      }
+    for (uint64_t i = tid; i < half; i += blockDim.x) {
+      const double u = A[i + half];
+      acc.add(u);
+      A[i] += u;
     }
-    double s = block_sum(acc.s);
-    if (tid == 0) out[1 + q] = s;
+    const double s = block_sum(acc.s);
+    if (tid == 0) out[1 + H + b] = s;
   }
 }
 

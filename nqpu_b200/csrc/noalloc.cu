@@ -28,7 +28,8 @@
 namespace nqpu {
 
 // Scratch bound: per-block partials (1024 x 16) + per-segment partials for
-// 2^27 128-bit vectors (32768 segments x 8) + the n+1 sums.
+// 2^27 128-bit vectors (32768 segments, room for 8 doubles each as the
+// reduction's scratch layout reserves) + the n+1 sums.
 constexpr int kNoAllocMaxVecLog2 = 27;
 constexpr size_t kNoAllocScratchDoubles = 1024 * 16 + (size_t(1) << (kNoAllocMaxVecLog2 - 12)) * 8 + 64;
 
