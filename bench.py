@@ -440,8 +440,11 @@ def run_batch(args):
     circs = [Circuit(n, g) for n, g, _, _ in items]
     host_build_s = time.perf_counter() - t0
     log = (lambda m: print(m, file=sys.stderr, flush=True)) if args.verbose else None
-    cfg, tune_report = autotune.tune(items, sample_size=min(args.tune_sample, count), circuits=circs,
-                                     use_cache=not args.no_tune_cache, log=log)
+    if args.quick:  # timed region only: library defaults, no tuning
+        cfg, tune_report = dict(autotune.DEFAULT), {"skipped": "--quick"}
+    else:
+        cfg, tune_report = autotune.tune(items, sample_size=min(args.tune_sample, count), circuits=circs,
+                                         use_cache=not args.no_tune_cache, log=log)
     b = Batch()
     b.config(**cfg)
     for c, (n, g, J, h) in zip(circs, items):
@@ -472,7 +475,7 @@ def run_batch(args):
 
     # the HBM-resident part of the work: 2S per pass tile sweep + S for <H>, S = 2^n * 8
     big_bytes = 0
-    sample = autotune.stratified_sample(items, min(args.plain_sample, count))
+    sample = autotune.stratified_sample(items, 0 if args.quick else min(args.plain_sample, count))
     for i in range(count):
         n = items[i][0]
         if n > cfg["small_max_qubits"]:
@@ -511,8 +514,8 @@ def run_batch(args):
         err_fp64 = max(err_fp64, abs(res[i] - e64) / scale)
     for s in states.values():
         s.close()
-    plain_rate = len(sample) / plain_s
-    tiled_rate = len(sample) / tiled_s
+    plain_rate = len(sample) / plain_s if sample else None
+    tiled_rate = len(sample) / tiled_s if sample else None
 
     # e2e through the public API: gate lists -> circuits -> batch -> <H> on the host
     e2e = None
@@ -553,7 +556,7 @@ def run_batch(args):
         "plain_per_circuit_path": {"circuits_per_s": plain_rate, "sample": len(sample),
                                    "what": "per-gate kernels + Pauli-sum <H>, one circuit at a time (host wall)"},
         "tiled_per_circuit_path": {"circuits_per_s": tiled_rate, "sample": len(sample)},
-        "speedup_vs_plain": value / plain_rate,
+        "speedup_vs_plain": value / plain_rate if plain_rate else None,
         "accuracy": {"max_rel_err_vs_fp64": err_fp64, "max_rel_err_vs_plain_c64": err_plain,
                      "tolerance": "|<H> - <H>_FP64| <= 1e-5 * (sum|J| + sum|h|)"},
         "host_build_s": host_build_s, "prepare_s": prepare_s, "wall_s_timed": wall,

@@ -71,6 +71,8 @@ def signature(items) -> str:
 
 def stratified_sample(items, size: int) -> list[int]:
     """Indices of every k-th circuit in (qubits, length) order."""
+    if size <= 0:
+        return []
     order = sorted(range(len(items)), key=lambda i: (items[i][0], len(items[i][1]), i))
     if size >= len(order):
         return order

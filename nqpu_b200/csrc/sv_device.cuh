@@ -48,6 +48,30 @@ __device__ __forceinline__ C cmac4(const C* m, C x0, C x1, C x2, C x3) {
   return r;
 }
 
+// Packed complex64 arithmetic (sm_100 FFMA2: one instruction on a float2
+// register pair).  A complex coefficient m is held as p = (re, re) and
+// q = (-im, im), so m * x = p * x + q * (x.im, x.re): two packed operations per
+// complex product instead of four scalar ones.  The swapped operand is always
+// the second multiplicand.
+struct PackedC {
+  float2 p, q;
+};
+__device__ __forceinline__ PackedC pack_coef(float2 m) {
+  return PackedC{make_float2(m.x, m.x), make_float2(-m.y, m.y)};
+}
+__device__ __forceinline__ float2 swap_ri(float2 v) { return make_float2(v.y, v.x); }
+// m * x
+__device__ __forceinline__ float2 pcmul(const PackedC& m, float2 x) {
+  return __ffma2_rn(m.q, swap_ri(x), __fmul2_rn(m.p, x));
+}
+// m0 * x + m1 * y (the 2x2 row product)
+__device__ __forceinline__ float2 pcmac2(const PackedC& m0, float2 x, const PackedC& m1, float2 y) {
+  float2 t = __fmul2_rn(m0.p, x);
+  t = __ffma2_rn(m0.q, swap_ri(x), t);
+  t = __ffma2_rn(m1.p, y, t);
+  return __ffma2_rn(m1.q, swap_ri(y), t);
+}
+
 __device__ __forceinline__ uint64_t insert_zero_bit(uint64_t v, int bit) {
   uint64_t lo = v & ((1ull << bit) - 1);
   return lo | ((v >> bit) << (bit + 1));

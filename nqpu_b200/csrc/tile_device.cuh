@@ -43,16 +43,35 @@ __device__ __forceinline__ void ldc2<double>(const double* __restrict__ p, doubl
   b = __ldg(reinterpret_cast<const double2*>(p) + 1);
 }
 
+// complex product on a register amplitude: packed FFMA2 form for complex64
+template <typename C>
+__device__ __forceinline__ C rmul(C m, C x) {
+  if constexpr (sizeof(m.x) == 4) return pcmul(pack_coef(m), x);
+  else return cmul(m, x);
+}
+
 // dense 2x2, no controls
 template <typename C, int NA, int B>
 __device__ __forceinline__ void rb_u1(C (&a)[NA], C m0, C m1, C m2, C m3) {
+  if constexpr (sizeof(m0.x) == 4) {
+    const PackedC p0 = pack_coef(m0), p1 = pack_coef(m1), p2 = pack_coef(m2), p3 = pack_coef(m3);
 #pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    if (i & (1 << B)) continue;
-    const int j = i | (1 << B);
-    const C x = a[i], y = a[j];
-    a[i] = cmac2(m0, x, m1, y);
-    a[j] = cmac2(m2, x, m3, y);
+    for (int i = 0; i < NA; ++i) {
+      if (i & (1 << B)) continue;
+      const int j = i | (1 << B);
+      const C x = a[i], y = a[j];
+      a[i] = pcmac2(p0, x, p1, y);
+      a[j] = pcmac2(p2, x, p3, y);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      if (i & (1 << B)) continue;
+      const int j = i | (1 << B);
+      const C x = a[i], y = a[j];
+      a[i] = cmac2(m0, x, m1, y);
+      a[j] = cmac2(m2, x, m3, y);
+    }
   }
 }
 
@@ -98,7 +117,7 @@ __device__ __forceinline__ void rb_ph(C (&a)[NA], C m, bool neg) {
       a[i].x = -a[i].x;
       a[i].y = -a[i].y;
     } else {
-      a[i] = cmul(m, a[i]);
+      a[i] = rmul(m, a[i]);
     }
   }
 }
@@ -109,10 +128,10 @@ __device__ __forceinline__ void rb_d1(C (&a)[NA], C d0, C d1, uint32_t tb) {
   if constexpr (DB >= NRB) {
     const C d = csel(tb != 0, d1, d0);
 #pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul(d, a[i]);
+    for (int i = 0; i < NA; ++i) a[i] = rmul(d, a[i]);
   } else {
 #pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul((i & (1 << DB)) ? d1 : d0, a[i]);
+    for (int i = 0; i < NA; ++i) a[i] = rmul((i & (1 << DB)) ? d1 : d0, a[i]);
   }
 }
 
@@ -124,22 +143,22 @@ __device__ __forceinline__ void rb_d2(C (&a)[NA], const C* m, uint32_t tb0, uint
     const C hi = csel(tb0 != 0, m[3], m[2]);
     const C d = csel(tb1 != 0, hi, lo);
 #pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul(d, a[i]);
+    for (int i = 0; i < NA; ++i) a[i] = rmul(d, a[i]);
   } else if constexpr (D0 >= NRB) {
     const C lo = csel(tb0 != 0, m[1], m[0]);
     const C hi = csel(tb0 != 0, m[3], m[2]);
 #pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul((i & (1 << D1)) ? hi : lo, a[i]);
+    for (int i = 0; i < NA; ++i) a[i] = rmul((i & (1 << D1)) ? hi : lo, a[i]);
   } else if constexpr (D1 >= NRB) {
     const C lo = csel(tb1 != 0, m[2], m[0]);
     const C hi = csel(tb1 != 0, m[3], m[1]);
 #pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = cmul((i & (1 << D0)) ? hi : lo, a[i]);
+    for (int i = 0; i < NA; ++i) a[i] = rmul((i & (1 << D0)) ? hi : lo, a[i]);
   } else {
 #pragma unroll
     for (int i = 0; i < NA; ++i) {
       const int k = ((i >> D0) & 1) | (((i >> D1) & 1) << 1);
-      a[i] = cmul(m[k], a[i]);
+      a[i] = rmul(m[k], a[i]);
     }
   }
 }
@@ -475,14 +494,24 @@ __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict
           // bit 0 stays bit 0: each vector keeps its pair, halves swap when
           // bit 0 of pi is flipped by the other register bits or by w
           const uint32_t h0 = m0 & 1u, h1 = m1 & 1u, h2 = m2 & 1u, h3 = m3 & 1u, hw = w & 1u;
+          if ((h0 | h1 | h2 | h3 | hw) == 0u) {
+            // no deferred flip of qubit 0 in this stage: whole vectors, no selects
 #pragma unroll
-          for (int r = 0; r < kVecPerThread; ++r) {
-            const uint32_t slot = sw ^ ((r & 1) ? c0 : 0u) ^ ((r & 2) ? c1 : 0u) ^
-                                  ((r & 4) ? c2 : 0u) ^ ((r & 8) ? c3 : 0u);
-            const uint32_t hs = hw ^ ((r & 1) ? h0 : 0u) ^ ((r & 2) ? h1 : 0u) ^
-                                ((r & 4) ? h2 : 0u) ^ ((r & 8) ? h3 : 0u);
-            const C lo = a[2 * r], hi = a[2 * r + 1];
-            sv[slot] = hs ? pack_vec<Real>(hi, lo) : pack_vec<Real>(lo, hi);
+            for (int r = 0; r < kVecPerThread; ++r) {
+              const uint32_t slot = sw ^ ((r & 1) ? c0 : 0u) ^ ((r & 2) ? c1 : 0u) ^
+                                    ((r & 4) ? c2 : 0u) ^ ((r & 8) ? c3 : 0u);
+              sv[slot] = pack_vec<Real>(a[2 * r], a[2 * r + 1]);
+            }
+          } else {
+#pragma unroll
+            for (int r = 0; r < kVecPerThread; ++r) {
+              const uint32_t slot = sw ^ ((r & 1) ? c0 : 0u) ^ ((r & 2) ? c1 : 0u) ^
+                                    ((r & 4) ? c2 : 0u) ^ ((r & 8) ? c3 : 0u);
+              const uint32_t hs = hw ^ ((r & 1) ? h0 : 0u) ^ ((r & 2) ? h1 : 0u) ^
+                                  ((r & 4) ? h2 : 0u) ^ ((r & 8) ? h3 : 0u);
+              const C lo = a[2 * r], hi = a[2 * r + 1];
+              sv[slot] = hs ? pack_vec<Real>(hi, lo) : pack_vec<Real>(lo, hi);
+            }
           }
         } else {
           // bit 0 moves into other bits: store each amplitude separately
