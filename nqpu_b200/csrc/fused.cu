@@ -18,6 +18,14 @@
 // TF32) and D = A_hi B_hi + A_hi B_lo + A_lo B_hi is accumulated in FP32 in
 // tensor memory by tcgen05.mma kind::tf32 (24 MMAs of 128x64x8 per tile).
 // Operands live in shared memory in the K-major 128-byte-swizzled layout.
+//
+// HBM access: a tile's 4096 amplitudes form a 12-dimensional sub-cube (F and
+// the 7 lowest qubits outside F, which always include qubits 0..6).  Loads and
+// stores walk the sub-cube in its own linear order, so each warp moves 512
+// contiguous bytes per 16-byte instruction; the (row, column) of every
+// amplitude in A (and D) follows from the same bits.  The output rows are
+// staged through shared memory to make the stores coalesced as well.  Two CTAs
+// share an SM, so one CTA's HBM traffic overlaps the other's MMAs.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -37,7 +45,6 @@ namespace nqpu {
 // Device kernel
 // ---------------------------------------------------------------------------
 constexpr int kFusedThreads = 128;         // one thread per group row (M = 128)
-constexpr int kRowBytes = 256;             // 64 fp32 per row
 constexpr int kAtomBytes = 128 * 128;      // one K-atom (32 tf32) of 128 rows
 constexpr int kAPlane = 2 * kAtomBytes;    // 32 KB: 128 rows x 64 tf32
 constexpr int kBPlane = 2 * 64 * 128;      // 16 KB: 64 rows x 64 tf32
@@ -51,7 +58,10 @@ struct FusedArgs {
   int ng;                 // number of group bits used
   int n_out;              // tile-id bits
   int qout[kMaxQubits];   // qubits of tile-id bits
-  int lane_over_j;        // 1: F contains qubit 0 (warp loads a group's amplitudes)
+  int lane_over_j;        // 1: F contains qubit 0
+  int sub[12];            // sub-cube qubits ascending (sub[0..6] = 0..6)
+  int sub_row[12];        // >= 0: row (group) bit of sub-cube bit b, else -1
+  int sub_col[12];        // >= 0: column (F) bit of sub-cube bit b, else -1
 };
 
 // Byte offset of element (row r, fp32 column k) in a K-major SW128 operand of
@@ -116,7 +126,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t phase) {
 // processed to out_norm[blockIdx.x]; the next launch sums those partials (in a
 // fixed order) and scales its own output by 1/sqrt(sum), so the norm drift of
 // each fused unitary is removed by the next one at no extra HBM pass.
-__global__ void __launch_bounds__(kFusedThreads, 1)
+constexpr int kFusedCtasPerSm = 2;
+
+__global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     k_fused_apply(float* __restrict__ amp, FusedArgs A, const float* __restrict__ bmat /* hi[64][64], lo[64][64] */,
                   const double* __restrict__ prev_norm, int n_prev, double* __restrict__ out_norm,
                   uint64_t n_tiles, int* __restrict__ err) {
@@ -129,8 +141,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   unsigned char* a_lo = base + kAPlane;
   unsigned char* b_hi = base + 2 * kAPlane;
   unsigned char* b_lo = b_hi + kBPlane;
-  uint64_t* gofs = reinterpret_cast<uint64_t*>(b_lo + kBPlane);   // 128 entries
-  uint64_t* fofs = gofs + 128;                                    // 32 entries
+  uint64_t* it_addr = reinterpret_cast<uint64_t*>(b_lo + kBPlane);  // 16 entries
+  uint32_t* it_rc = reinterpret_cast<uint32_t*>(it_addr + 16);        // 16 entries: row | col << 16
+  float2* stage = reinterpret_cast<float2*>(a_hi);                    // output staging (reuses A_hi)
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_holder;
   __shared__ int abort_flag;
@@ -138,18 +151,34 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t mbar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar));
 
-  // offset tables
-  if (tid < 128) {
-    uint64_t o = 0;
-    for (int b = 0; b < A.ng; ++b)
-      if ((tid >> b) & 1) o |= 1ull << A.gq[b];
-    gofs[tid] = o;
+  // Sub-cube index u = h | tid << 1 | i << 8 (h: amplitude in a 16-byte pair,
+  // i: load step).  Global offset, row and column of u are XORs of the parts.
+  auto part = [&](uint32_t u, uint64_t* addr, uint32_t* row, uint32_t* col) {
+    uint64_t a = 0;
+    uint32_t r = 0, c = 0;
+    for (int b = 0; b < 12; ++b)
+      if ((u >> b) & 1u) {
+        a |= 1ull << A.sub[b];
+        if (A.sub_row[b] >= 0) r |= 1u << A.sub_row[b];
+        else c |= 1u << A.sub_col[b];
+      }
+    *addr = a;
+    *row = r;
+    *col = c;
+  };
+  if (tid < 16) {
+    uint64_t a;
+    uint32_t r, c;
+    part(uint32_t(tid) << 8, &a, &r, &c);
+    it_addr[tid] = a;
+    it_rc[tid] = r | (c << 16);
   }
-  if (tid < 32) {
-    uint64_t o = 0;
-    for (int b = 0; b < 5; ++b)
-      if ((tid >> b) & 1) o |= 1ull << A.q[b];
-    fofs[tid] = o;
+  uint64_t t_addr;
+  uint32_t t_row, t_col, h_row, h_col;
+  {
+    uint64_t a;
+    part(uint32_t(tid) << 1, &t_addr, &t_row, &t_col);
+    part(1u, &a, &h_row, &h_col);
   }
   // B operand (constant for the launch): row n (output real index), col k
   for (int i = tid; i < 64 * 64; i += blockDim.x) {
@@ -185,30 +214,41 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const uint32_t blo_s = static_cast<uint32_t>(__cvta_generic_to_shared(b_lo));
 
   uint32_t phase = 0;
-  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  auto tile_base_of = [&](uint64_t tile) {
     uint64_t tb = 0;
     for (int j = 0; j < A.n_out; ++j)
       if ((tile >> j) & 1ull) tb |= 1ull << A.qout[j];
-    const float2* src = reinterpret_cast<const float2*>(amp) + tb;
-
-    // HBM -> A_hi / A_lo (split), swizzled K-major rows
-    auto put = [&](uint32_t row, uint32_t j, float2 v) {
-      const uint32_t o0 = sw128_off<128>(row, 2 * j), o1 = sw128_off<128>(row, 2 * j + 1);
-      const float hr = tf32_rn(v.x), hi_ = tf32_rn(v.y);
-      *reinterpret_cast<float*>(a_hi + o0) = hr;
-      *reinterpret_cast<float*>(a_hi + o1) = hi_;
-      *reinterpret_cast<float*>(a_lo + o0) = tf32_rn(v.x - hr);
-      *reinterpret_cast<float*>(a_lo + o1) = tf32_rn(v.y - hi_);
-    };
-    if (A.lane_over_j) {
-      // a warp reads the 32 amplitudes of one group per step (qubit 0 is in F)
-      for (int g = warp; g < 128; g += kFusedThreads / 32) put(g, lane, __ldcs(src + gofs[g] + fofs[lane]));
-    } else {
-      float2 v[32];
+    return tb;
+  };
+  // tile base tb has no sub-cube bits, and sub-cube bit 0 is qubit 0, so the
+  // pair (u, u + 1) is one 16-byte-aligned float4
+  auto load_tile = [&](uint64_t tb, float4 (&v)[16]) {
+    const float4* src4 = reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(amp) + tb + t_addr);
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = __ldcs(src + gofs[tid] + fofs[j]);
+    for (int i = 0; i < 16; ++i) v[i] = __ldcs(src4 + (it_addr[i] >> 1));
+  };
+  // HBM -> A_hi / A_lo (split), swizzled K-major rows; (re, im) = columns
+  // (2j, 2j + 1) share one aligned 8-byte slot of a 16-byte chunk
+  auto put = [&](uint32_t row, uint32_t j, float re, float im) {
+    const uint32_t o0 = sw128_off<128>(row, 2 * j);
+    const float hr = tf32_rn(re), hi_ = tf32_rn(im);
+    *reinterpret_cast<float2*>(a_hi + o0) = make_float2(hr, hi_);
+    *reinterpret_cast<float2*>(a_lo + o0) = make_float2(tf32_rn(re - hr), tf32_rn(im - hi_));
+  };
+  // software pipeline: the next tile's HBM loads are in flight while the
+  // current tile's MMAs, epilogue and stores run
+  float4 v[16];
+  if (uint64_t(blockIdx.x) < n_tiles) load_tile(tile_base_of(blockIdx.x), v);
+  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const uint64_t tb = tile_base_of(tile);
+    {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) put(tid, j, v[j]);
+      for (int i = 0; i < 16; ++i) {
+        const uint32_t rc = it_rc[i];
+        const uint32_t r0 = t_row | (rc & 0xFFFFu), c0 = t_col | (rc >> 16);
+        put(r0, c0, v[i].x, v[i].y);
+        put(r0 | h_row, c0 | h_col, v[i].z, v[i].w);
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -229,6 +269,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_addr)
                    : "memory");
     }
+    if (tile + gridDim.x < n_tiles) load_tile(tile_base_of(tile + gridDim.x), v);
     // bounded wait for the MMAs
     {
       uint32_t it = 0;
@@ -265,26 +306,38 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 
-    float2* dst = reinterpret_cast<float2*>(amp) + tb + gofs[tid];
+    // row tid of D -> staging (row-major, column index XOR-swizzled by row)
     double tile_norm = 0.0;
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const float2 o = make_float2(__uint_as_float(r[2 * j]) * scale, __uint_as_float(r[2 * j + 1]) * scale);
       tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
-      __stcs(dst + fofs[j], o);
+      stage[tid * 32 + (j ^ (tid & 31))] = o;
     }
     norm_acc += tile_norm;
-
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();  // TMEM and the A planes are reused by the next tile
+    __syncthreads();  // staging complete; TMEM free for the next tile
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    {
+      float4* dst4 = reinterpret_cast<float4*>(reinterpret_cast<float2*>(amp) + tb + t_addr);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const uint32_t rc = it_rc[i];
+        const uint32_t r0 = t_row | (rc & 0xFFFFu), c0 = t_col | (rc >> 16);
+        const uint32_t r1 = r0 | h_row, c1 = c0 | h_col;
+        const float2 o0 = stage[r0 * 32 + (c0 ^ (r0 & 31))];
+        const float2 o1 = stage[r1 * 32 + (c1 ^ (r1 & 31))];
+        __stcs(dst4 + (it_addr[i] >> 1), make_float4(o0.x, o0.y, o1.x, o1.y));
+      }
+    }
+    __syncthreads();  // the A planes (and the staging area in A_hi) are refilled next tile
   }
   // per-CTA FP64 norm partial (fixed-order tree: warp shuffles, then warp 0)
   __shared__ double wsum[kFusedThreads / 32];
-  double v = norm_acc;
+  double nsum = norm_acc;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0) wsum[warp] = v;
+  for (int o = 16; o > 0; o >>= 1) nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
+  if (lane == 0) wsum[warp] = nsum;
   __syncthreads();
   if (tid == 0) {
     double t = 0.0;
@@ -346,6 +399,22 @@ static FusedArgs make_args(const FusedGate& g, int n) {
     if (!(((F | G) >> q) & 1)) a.qout[no++] = q;
   a.n_out = no;
   a.lane_over_j = (F & 1ull) ? 1 : 0;
+  // sub-cube bits in ascending qubit order
+  int nb = 0;
+  for (int q = 0; q < n && nb < 12; ++q) {
+    if (!(((F | G) >> q) & 1)) continue;
+    a.sub[nb] = q;
+    a.sub_row[nb] = -1;
+    a.sub_col[nb] = -1;
+    if ((F >> q) & 1) {
+      for (int i = 0; i < 5; ++i)
+        if (a.q[i] == q) a.sub_col[nb] = i;
+    } else {
+      for (int i = 0; i < ng; ++i)
+        if (a.gq[i] == q) a.sub_row[nb] = i;
+    }
+    ++nb;
+  }
   return a;
 }
 
@@ -374,7 +443,7 @@ bool fused_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, 
   }
   bool ok = cudaMalloc(reinterpret_cast<void**>(&p->d_bmats), host.size() * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMemcpy(p->d_bmats, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess;
-  p->norm_slots = device_sms();
+  p->norm_slots = device_sms() * kFusedCtasPerSm;
   ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_norm), sizeof(double) * 2 * p->norm_slots) == cudaSuccess;
   ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_err), sizeof(int)) == cudaSuccess;
   ok = ok && cudaMemset(p->d_err, 0, sizeof(int)) == cudaSuccess;

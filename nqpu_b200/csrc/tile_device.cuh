@@ -271,10 +271,25 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
                                                 const TileOp<Real>* __restrict__ ops, int ob,
                                                 int oe, uint32_t vbase) {
   using C = typename Tr<Real>::C;
+  // software pipeline: the next op's header and first four matrix entries are
+  // loaded while the current op runs
+  uint4 nh = make_uint4(0, 0, 0, 0);
+  uint32_t ndv1 = 0;
+  C nm[4];
+  auto fetch = [&](int o) {
+    const TileOp<Real>* op = ops + o;
+    nh = __ldg(reinterpret_cast<const uint4*>(op));
+    ndv1 = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
+    ldc2<Real>(op->m, nm[0], nm[1]);
+    ldc2<Real>(op->m + 4, nm[2], nm[3]);
+  };
+  if (ob < oe) fetch(ob);
   for (int o = ob; o < oe; ++o) {
     const TileOp<Real>* op = ops + o;
-    const uint4 h0 = __ldg(reinterpret_cast<const uint4*>(op));
-    const uint32_t dv1 = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
+    const uint4 h0 = nh;
+    const uint32_t dv1 = ndv1;
+    const C pm0 = nm[0], pm1 = nm[1], pm2 = nm[2], pm3 = nm[3];
+    if (o + 1 < oe) fetch(o + 1);
     const uint32_t kind = h0.x & 0xFF;
     const uint32_t rb0 = (h0.x >> 8) & 0xFF;
     const uint32_t rb1 = (h0.x >> 16) & 0xFF;
@@ -287,9 +302,7 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
     const Real* mp = op->m;
     switch (kind) {
       case OP_U1: {
-        C m0, m1, m2, m3;
-        ldc2<Real>(mp, m0, m1);
-        ldc2<Real>(mp + 4, m2, m3);
+        const C m0 = pm0, m1 = pm1, m2 = pm2, m3 = pm3;
         if (creg == 0) {
           if (!tc) break;
           switch (rb0) {
@@ -318,15 +331,15 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
       }
       case OP_PH: {
         if (!tc) break;
-        C m0, m1;
-        ldc2<Real>(mp, m0, m1);
+        const C m0 = pm0;
         const bool neg = (m0.x == Real(-1)) && (m0.y == Real(0));
         dispatch_ph<C, NA, NRB>(a, creg, m0, neg);
         break;
       }
       case OP_D1: {
         C m[4];
-        ldc2<Real>(mp, m[0], m[1]);
+        m[0] = pm0;
+        m[1] = pm1;
         const uint32_t tb = (vbase & dv0) ? 1u : 0u;
         if (creg == 0 && cnr == 0) {
           switch (dreg0 == 0xFF ? NRB : int(dreg0)) {
@@ -344,9 +357,7 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
         break;
       }
       case OP_D2: {
-        C m[4];
-        ldc2<Real>(mp, m[0], m[1]);
-        ldc2<Real>(mp + 4, m[2], m[3]);
+        C m[4] = {pm0, pm1, pm2, pm3};
         const uint32_t tb0 = (vbase & dv0) ? 1u : 0u;
         const uint32_t tb1 = (vbase & dv1) ? 1u : 0u;
         if (creg == 0 && cnr == 0) {
