@@ -260,8 +260,10 @@ NqpuError    nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* stat
 NqpuError    nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,
                                   float* launch_ms, uint32_t len, uint32_t* count);
 /* Tiled-pass kernel configuration per dtype: ctas_per_sm = 1 (one CTA per SM,
- * double-buffered tiles) or 2 (two CTAs per SM, single-buffered).  Set by the
- * autotuner; applies to launches made after the call. */
+ * double-buffered 64 KB tiles), 2 (two CTAs per SM, single-buffered 64 KB
+ * tiles) or 4 (four CTAs per SM on 32 KB tiles, one tile qubit fewer).  Plans
+ * are built for the configuration in force when a circuit is first run on a
+ * state size (a plan built for larger tiles is rebuilt, never run on smaller). */
 NqpuError    nqpu_tile_config_set(NqpuDtype dtype, uint32_t ctas_per_sm);
 uint32_t     nqpu_tile_config_get(NqpuDtype dtype);
 /* Plan statistics of the last execution of `circuit` in `mode` on an n-qubit state:

@@ -660,7 +660,7 @@ extern "C" NqpuError nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_
 }
 
 extern "C" NqpuError nqpu_tile_config_set(NqpuDtype dtype, uint32_t ctas_per_sm) {
-  if (ctas_per_sm != 1 && ctas_per_sm != 2) return NQPU_INVALID_PARAMETER;
+  if (ctas_per_sm != 1 && ctas_per_sm != 2 && ctas_per_sm != 4) return NQPU_INVALID_PARAMETER;
   tile_config_set(dtype == NQPU_C64 ? DType::C64 : DType::C128, int(ctas_per_sm));
   return NQPU_OK;
 }

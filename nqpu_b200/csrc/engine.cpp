@@ -224,7 +224,8 @@ static bool plan_host(const CircuitImpl* c, uint32_t n, DType dt, int mode, Devi
   p->stats = PlanStats{};
   if (mode == NQPU_MODE_TILED && int(n) >= tile_min_qubits(dt)) {
     std::string err;
-    if (!build_tile_plan(p->ops, int(n), dt, tile_kmax_for(dt), &p->tile, &err)) return false;
+    p->kmax = tile_kmax_for(dt);
+    if (!build_tile_plan(p->ops, int(n), dt, p->kmax, &p->tile, &err)) return false;
     p->stats = p->tile.stats;
   } else if (mode == NQPU_MODE_FUSED) {
     p->stats.ops = p->ops.size();
@@ -289,7 +290,8 @@ cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cuda
   const int effective = (mode == NQPU_MODE_TILED && int(s->n) < tile_min_qubits(s->dt)) ? int(NQPU_MODE_PERGATE) : mode;
   const auto key = std::make_tuple(s->n, int(s->dt), effective);
   DevicePlan*& p = c->plans[key];
-  if (p && p->version != c->version) {
+  // rebuild when the circuit changed or the tiled kernel's tile size did
+  if (p && (p->version != c->version || (effective == NQPU_MODE_TILED && p->kmax != tile_kmax_for(s->dt)))) {
     cudaStreamSynchronize(s->stream);
     plan_free(p);
     p = nullptr;

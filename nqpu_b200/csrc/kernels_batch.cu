@@ -121,9 +121,11 @@ __global__ void __launch_bounds__(kTileThreads, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* sv = reinterpret_cast<float4*>(smem_raw);
   uint64_t* hi_off = reinterpret_cast<uint64_t*>(smem_raw + sizeof(float4) * kBatchVec);
-  double* lut = reinterpret_cast<double*>(hi_off + 1024);  // 3 x 256 bond-sum tables
-  double* hq = lut + 768;                                  // h_i, i < n
+  double* lut = reinterpret_cast<double*>(hi_off + kHiOffEntries);  // 3 x 256 bond-sum tables
+  double* hq = lut + 768;                                           // h_i, i < n
+  uint32_t* tabs = reinterpret_cast<uint32_t*>(hq + 64);            // stage tables of the current pass
   __shared__ PassRec P;
+  __shared__ int s_pass;  // global index of the pass whose tables are loaded (-1: none)
   __shared__ uint32_t s_task;
   __shared__ int s_flag;
   __shared__ double red[kTileThreads / 32];
@@ -150,8 +152,12 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     for (uint32_t u = tid; u < nvec; u += blockDim.x)
       sv[swz(u)] = (one && u == 0) ? make_float4(1.f, 0.f, 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
   };
+  // Pass record, high-offset table and stage tables; consecutive tasks of the
+  // same pass on this CTA reuse them.
   auto load_pass = [&](const BatchCirc& C, int p) {
-    const int32_t* src = reinterpret_cast<const int32_t*>(passes + C.pass_base + p);
+    const int gp = C.pass_base + p;
+    if (s_pass == gp) return;  // uniform: every thread read s_pass after the last barrier
+    const int32_t* src = reinterpret_cast<const int32_t*>(passes + gp);
     int32_t* dst = reinterpret_cast<int32_t*>(&P);
     for (int i = tid; i < int(sizeof(PassRec) / 4); i += blockDim.x) dst[i] = src[i];
     __syncthreads();
@@ -162,8 +168,12 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         if ((hh >> j) & 1) off |= 1ull << P.qhi[j];
       hi_off[hh] = off;
     }
+    build_pass_tabs<float>(P, stages, tabs);  // ends with a barrier
+    if (tid == 0) s_pass = gp;
     __syncthreads();
   };
+  if (tid == 0) s_pass = -1;
+  __syncthreads();
 
   for (;;) {
     if (tid == 0) {
@@ -183,7 +193,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       const uint32_t nvec = 1u << (P.k - 1);
       init_tile(nvec, true);
       __syncthreads();
-      run_tile_stages<float>(sv, P, stages, ops, 0u);
+      run_tile_stages<float>(sv, P, tabs, ops, 0u);
       double jtot;
       load_obs(C, &jtot);
       __syncthreads();
@@ -221,7 +231,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         cp_async_wait0();
       }
       __syncthreads();
-      run_tile_stages<float>(sv, P, stages, ops, ext);
+      run_tile_stages<float>(sv, P, tabs, ops, ext);
       for (uint32_t u = tid; u < nvec; u += blockDim.x) {
         const uint32_t t = u << 1;
         const uint64_t g = base + (t & lowmask) + hi_off[t >> c];
@@ -265,7 +275,10 @@ __global__ void __launch_bounds__(kTileThreads, 2)
   }
 }
 
-size_t batch_smem_bytes() { return sizeof(float4) * kBatchVec + sizeof(uint64_t) * 1024 + sizeof(double) * (768 + 64); }
+size_t batch_smem_bytes() {
+  return sizeof(float4) * kBatchVec + sizeof(uint64_t) * kHiOffEntries + sizeof(double) * (768 + 64) +
+         sizeof(uint32_t) * kMaxPassStages * kStageTabWords;
+}
 
 cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s) {
   static bool configured = false;

@@ -22,11 +22,14 @@
 
 namespace nqpu {
 
-// Dynamic shared memory: [tile buffer 0 | tile buffer 1 | hi_off table (2^(k-c) u64)].
-// One persistent CTA per SM: while the stages of tile i run on one buffer, the
-// cp.async copies of tile i+1 stream into the other.
+// Dynamic shared memory: [tile buffer 0 | tile buffer 1 | hi_off table
+// (2^(k-c) <= kHiOffEntries u64) | stage tables (kMaxPassStages x kStageTabWords u32)].
+// MINB = 1: one persistent CTA per SM; while the stages of tile i run on one
+// buffer, the cp.async copies of tile i+1 stream into the other.  MINB > 1:
+// MINB CTAs per SM with one buffer each hide each other's copies.  Each thread
+// holds 16 vectors, so a CTA has 2^KMAX / (16 x amplitudes per vector) threads.
 template <typename Real, int KMAX, int MINB>
-__global__ void __launch_bounds__(kTileThreads, MINB)
+__global__ void __launch_bounds__(1 << (KMAX - Tr<Real>::kVecBit - 4), MINB)
     k_tile_pass(Real* __restrict__ amp, const PassRec* __restrict__ passes,
                 const StageRec* __restrict__ stages, const TileOp<Real>* __restrict__ ops,
                 int pass_idx, uint64_t n_tiles) {
@@ -34,12 +37,14 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
   using V = typename T::V;
   constexpr int VB = T::kVecBit;
   constexpr uint32_t kMaxVec = 1u << (KMAX - VB);
+  constexpr int kThreads = int(kMaxVec) / kVecPerThread;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr bool kDoubleBuffer = (MINB == 1);
   V* buf0 = reinterpret_cast<V*>(smem_raw);
   V* buf1 = kDoubleBuffer ? buf0 + kMaxVec : buf0;
   uint64_t* hi_off = reinterpret_cast<uint64_t*>(smem_raw + (kDoubleBuffer ? 2 : 1) * sizeof(V) * kMaxVec);
+  uint32_t* tabs = reinterpret_cast<uint32_t*>(hi_off + kHiOffEntries);
   __shared__ PassRec P;
 
   const int tid = threadIdx.x;
@@ -58,7 +63,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
       if ((h >> j) & 1) off |= 1ull << P.qhi[j];
     hi_off[h] = off;
   }
-  __syncthreads();
+  build_pass_tabs<Real>(P, stages, tabs);  // ends with a barrier
   const uint32_t lowmask = (1u << c) - 1u;
 
   // HBM -> shared, asynchronous (consecutive threads take consecutive vectors).
@@ -66,7 +71,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     const uint64_t base = tile_base(P, tile);
 #pragma unroll
     for (int i = 0; i < kVecPerThread; ++i) {
-      const uint32_t u = tid + i * kTileThreads;
+      const uint32_t u = tid + i * kThreads;
       if (u < nvec) {
         const uint32_t t = u << VB;
         const uint64_t g = base + (t & lowmask) + hi_off[t >> c];
@@ -98,12 +103,12 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     for (int j = 0; j < P.n_ext; ++j)
       if ((base >> P.ext[j]) & 1ull) ext |= 1u << (k + j);
 
-    run_tile_stages<Real>(sv, P, stages, ops, ext);
+    run_tile_stages<Real>(sv, P, tabs, ops, ext);
 
     // shared -> HBM
 #pragma unroll
     for (int i = 0; i < kVecPerThread; ++i) {
-      const uint32_t u = tid + i * kTileThreads;
+      const uint32_t u = tid + i * kThreads;
       if (u < nvec) {
         const uint32_t t = u << VB;
         const uint64_t g = base + (t & lowmask) + hi_off[t >> c];
@@ -114,28 +119,46 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
   }
 }
 
+// Largest tile (bits) per dtype: 64 KB of amplitudes.
 template <typename Real>
+constexpr int tile_kmax_full() { return sizeof(Real) == 4 ? 13 : 12; }
+
+template <typename Real, int KMAX>
 static size_t tile_smem_bytes(int minb) {
   using V = typename Tr<Real>::V;
-  const int kmax = sizeof(Real) == 4 ? 13 : 12;
-  return (minb == 1 ? 2 : 1) * sizeof(V) * (size_t(1) << (kmax - Tr<Real>::kVecBit)) + sizeof(uint64_t) * 1024;
+  return (minb == 1 ? 2 : 1) * sizeof(V) * (size_t(1) << (KMAX - Tr<Real>::kVecBit)) +
+         sizeof(uint64_t) * kHiOffEntries + sizeof(uint32_t) * kMaxPassStages * kStageTabWords;
 }
 
-// CTA configuration of the tiled pass kernel: 1 = one CTA per SM with a
-// double-buffered tile (cp.async prefetch of the next tile), 2 = two CTAs per
-// SM with one tile buffer each.  Chosen by tile_config_set (the autotuner).
-static int g_tile_minb[2] = {2, 2};
+// CTA configuration of the tiled pass kernel per dtype (CTAs per SM):
+//   1: one 64 KB-tile CTA per SM, double-buffered (cp.async prefetch of the next tile);
+//   2: two 64 KB-tile CTAs per SM, one buffer each;
+//   4: four CTAs per SM on 32 KB tiles (one tile bit fewer, half the threads):
+//      more independent CTAs to overlap each other's barriers and copies, at
+//      the price of more passes.
+// Plans are built for the configuration's tile size (tile_kmax_for).
+// Defaults measured on B200 (28-qubit brickwork): complex64 runs fastest with
+// four 32 KB-tile CTAs per SM, complex128 with one double-buffered CTA (its
+// 2-CTA build spills registers).
+static int g_tile_minb[2] = {4, 1};
 
-void tile_config_set(DType dt, int minb) { g_tile_minb[dt == DType::C64 ? 0 : 1] = (minb == 2) ? 2 : 1; }
+void tile_config_set(DType dt, int minb) {
+  g_tile_minb[dt == DType::C64 ? 0 : 1] = (minb == 4) ? 4 : (minb == 2) ? 2 : 1;
+}
 int tile_config_get(DType dt) { return g_tile_minb[dt == DType::C64 ? 0 : 1]; }
 
-template <typename Real, int MINB>
+template <typename Real, int KMAX, int MINB>
 cudaError_t launch_tile_pass_cfg(Real* amp, const PassRec& host_pass, const PassRec* d_passes,
                                  const StageRec* d_stages, const TileOp<Real>* d_ops, int pass_idx,
                                  cudaStream_t stream, int num_sms) {
-  constexpr int KMAX = sizeof(Real) == 4 ? 13 : 12;
+  // a plan built for larger tiles than this kernel holds must not run on it,
+  // nor one whose tables exceed the shared-memory copies
+  if (host_pass.k > KMAX || host_pass.k < 1 || host_pass.k - host_pass.c > kHiOffBits ||
+      host_pass.stage_end - host_pass.stage_begin > kMaxPassStages)
+    return cudaErrorInvalidValue;
   auto kern = k_tile_pass<Real, KMAX, MINB>;
-  const size_t smem = tile_smem_bytes<Real>(MINB);
+  constexpr int kThreads = (1 << (KMAX - Tr<Real>::kVecBit)) / kVecPerThread;
+  const size_t smem = tile_smem_bytes<Real, KMAX>(MINB);
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -145,7 +168,7 @@ cudaError_t launch_tile_pass_cfg(Real* amp, const PassRec& host_pass, const Pass
   const uint64_t n_tiles = 1ull << host_pass.n_out;
   const uint64_t max_ctas = uint64_t(num_sms) * MINB;
   const unsigned grid = unsigned(n_tiles < max_ctas ? n_tiles : max_ctas);
-  kern<<<grid, kTileThreads, smem, stream>>>(amp, d_passes, d_stages, d_ops, pass_idx, n_tiles);
+  kern<<<grid, kThreads, smem, stream>>>(amp, d_passes, d_stages, d_ops, pass_idx, n_tiles);
   return cudaGetLastError();
 }
 
@@ -154,9 +177,16 @@ cudaError_t launch_tile_pass_t(Real* amp, int n, const PassRec& host_pass, const
                                const StageRec* d_stages, const TileOp<Real>* d_ops, int pass_idx,
                                cudaStream_t stream, int num_sms) {
   (void)n;
-  if (g_tile_minb[sizeof(Real) == 4 ? 0 : 1] == 2)
-    return launch_tile_pass_cfg<Real, 2>(amp, host_pass, d_passes, d_stages, d_ops, pass_idx, stream, num_sms);
-  return launch_tile_pass_cfg<Real, 1>(amp, host_pass, d_passes, d_stages, d_ops, pass_idx, stream, num_sms);
+  constexpr int K = tile_kmax_full<Real>();
+  switch (g_tile_minb[sizeof(Real) == 4 ? 0 : 1]) {
+    case 4:
+      return launch_tile_pass_cfg<Real, K - 1, 4>(amp, host_pass, d_passes, d_stages, d_ops, pass_idx, stream,
+                                                  num_sms);
+    case 2:
+      return launch_tile_pass_cfg<Real, K, 2>(amp, host_pass, d_passes, d_stages, d_ops, pass_idx, stream, num_sms);
+    default:
+      return launch_tile_pass_cfg<Real, K, 1>(amp, host_pass, d_passes, d_stages, d_ops, pass_idx, stream, num_sms);
+  }
 }
 
 cudaError_t launch_tile_pass(DType dt, void* amp, int n, const PassRec& host_pass,
@@ -171,6 +201,9 @@ cudaError_t launch_tile_pass(DType dt, void* amp, int n, const PassRec& host_pas
                                     num_sms);
 }
 
-int tile_kmax_for(DType dt) { return dt == DType::C64 ? 13 : 12; }
+int tile_kmax_for(DType dt) {
+  const int full = dt == DType::C64 ? 13 : 12;
+  return tile_config_get(dt) == 4 ? full - 1 : full;
+}
 
 }  // namespace nqpu

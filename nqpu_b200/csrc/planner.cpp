@@ -15,6 +15,7 @@
 #include "planner.h"
 #include <algorithm>
 #include <cmath>
+#include <iterator>
 #include <cstring>
 
 namespace nqpu {
@@ -350,7 +351,21 @@ bool build_tile_plan(const std::vector<Op>& ops, int n, DType dt, int kmax, Tile
       return tile_pos[q] >= 0 ? (1u << tile_pos[q]) : (1u << (k + ext_of_qubit[q]));
     };
     std::vector<int> pending = taken;
+    int pass_stages = 0;
     while (!pending.empty()) {
+      if (pass_stages == kMaxPassStages) {
+        // stage cap reached: the ops not yet placed go back, in circuit
+        // order, ahead of the ops this pass left out (they commute with every
+        // earlier left-out op, or they would not have been taken)
+        std::sort(pending.begin(), pending.end());
+        std::vector<int> merged;
+        merged.reserve(pending.size() + rest.size());
+        std::merge(pending.begin(), pending.end(), rest.begin(), rest.end(), std::back_inserter(merged));
+        rest.swap(merged);
+        pending.clear();
+        break;
+      }
+      ++pass_stages;
       uint64_t R = 0;          // tile-bit mask of free register bits
       uint64_t no_reg = 0;     // tile bits that must stay thread-level in this stage
       uint64_t sblocked = 0;   // qubits blocked for the rest of the stage

@@ -104,6 +104,10 @@ struct PassRec {
 // conditional translation i applies w = cond_w[i] when the amplitude's virtual
 // index has all bits cond_cnr[i] set (a control outside the register bits).
 constexpr int kMaxCondPerm = 4;
+// Stages per pass are capped so that the kernels can keep every stage's
+// derived constants of a pass in shared memory (kStageTabWords words each).
+constexpr int kMaxPassStages = 48;
+constexpr int kStageTabWords = 96;
 
 struct StageRec {
   int32_t rpos[kRegFree];    // tile-local bit positions of the free register bits

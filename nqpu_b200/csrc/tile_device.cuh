@@ -8,6 +8,10 @@ namespace nqpu {
 
 constexpr int kTileThreads = 256;
 constexpr int kVecPerThread = 16;
+// Tile bits above the contiguous low block: k - c <= 8 (c >= 5 for complex64,
+// c >= 4 for complex128, k <= 13 / 12), so the high-offset table has <= 256 entries.
+constexpr int kHiOffBits = 8;
+constexpr int kHiOffEntries = 1 << kHiOffBits;
 
 __device__ __forceinline__ uint32_t swz(uint32_t u) {
   uint32_t w = u >> 3;
@@ -59,9 +63,15 @@ __device__ __forceinline__ void rb_u1(C (&a)[NA], C m0, C m1, C m2, C m3) {
     for (int i = 0; i < NA; ++i) {
       if (i & (1 << B)) continue;
       const int j = i | (1 << B);
-      const C x = a[i], y = a[j];
-      a[i] = pcmac2(p0, x, p1, y);
-      a[j] = pcmac2(p2, x, p3, y);
+      const float2 x = a[i], y = a[j];
+      const float2 sx = swap_ri(x), sy = swap_ri(y);
+      float2 ti = __fmul2_rn(p0.p, x), tj = __fmul2_rn(p2.p, x);
+      ti = __ffma2_rn(p0.q, sx, ti);
+      tj = __ffma2_rn(p2.q, sx, tj);
+      ti = __ffma2_rn(p1.p, y, ti);
+      tj = __ffma2_rn(p3.p, y, tj);
+      a[i] = __ffma2_rn(p1.q, sy, ti);
+      a[j] = __ffma2_rn(p3.q, sy, tj);
     }
   } else {
 #pragma unroll
@@ -442,12 +452,93 @@ __device__ __forceinline__ uint64_t tile_base(const PassRec& P, uint64_t tile) {
 }
 
 
+// Per-stage constants derived from a StageRec, kept in shared memory for the
+// whole pass (kStageTabWords words per stage; built once per pass by
+// build_stage_tab, so the per-tile stage loop does no bit-by-bit work):
+//   S..S+3     slot offsets swz(vector bit of free register bit i)
+//   CW..CW+3   slot offsets of the write-back images of the free register bits
+//   HB         bit i: the image of free register bit i flips amplitude bit 0 (complex64)
+//   MZ         image of register bit 0 (complex64; 1 = bit 0 stays bit 0)
+//   CZ, HZ     slot offset and bit 0 of MZ's image
+//   WS, WH     slot offset and bit 0 of the constant translation sbx
+//   NC, OB, OE conditional translations, op range
+//   CC, CS, CH per conditional translation: control mask, slot offset, bit 0
+//   UL, UH     deposit of thread-index bits 0..3 / 4..7 into the vector index
+//   SL, SH     the same deposits through the swizzle (swz is linear over XOR)
+struct StageTab {
+  enum : int { S = 0, CW = 4, HB = 8, MZ = 9, CZ = 10, HZ = 11, WS = 12, WH = 13, NC = 14, OB = 15, OE = 16,
+               CC = 17, CS = 21, CH = 25, UL = 32, UH = 48, SL = 64, SH = 80 };
+};
+static_assert(StageTab::SH + 16 <= kStageTabWords, "stage table layout");
+
+template <int VB>
+__device__ void build_stage_tab(const StageRec* __restrict__ S, uint32_t* __restrict__ t) {
+  uint32_t s[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s[i] = swz(1u << (S->rpos[i] - VB));
+  auto regslot = [&](uint32_t m) {
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if ((m >> (VB + i)) & 1u) x ^= s[i];
+    return x;
+  };
+  uint32_t hb = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t m = uint32_t(S->scol[VB + i]);
+    t[StageTab::S + i] = s[i];
+    t[StageTab::CW + i] = regslot(m);
+    hb |= (VB == 1 ? (m & 1u) : 0u) << i;
+  }
+  const uint32_t mz = VB == 1 ? uint32_t(S->scol[0]) : 1u;
+  t[StageTab::HB] = hb;
+  t[StageTab::MZ] = mz;
+  t[StageTab::CZ] = regslot(mz);
+  t[StageTab::HZ] = VB == 1 ? (mz & 1u) : 0u;
+  t[StageTab::WS] = regslot(uint32_t(S->sbx));
+  t[StageTab::WH] = VB == 1 ? (uint32_t(S->sbx) & 1u) : 0u;
+  t[StageTab::NC] = uint32_t(S->ncond);
+  t[StageTab::OB] = uint32_t(S->op_begin);
+  t[StageTab::OE] = uint32_t(S->op_end);
+  for (int i = 0; i < kMaxCondPerm; ++i) {
+    const uint32_t w = uint32_t(S->cond_w[i]);
+    t[StageTab::CC + i] = S->cond_cnr[i];
+    t[StageTab::CS + i] = regslot(w);
+    t[StageTab::CH + i] = VB == 1 ? (w & 1u) : 0u;
+  }
+  const int ntb = S->n_tbits;
+  for (int v = 0; v < 16; ++v) {
+    uint32_t lo = 0, hi = 0;
+    for (int j = 0; j < 4; ++j) {
+      if (j < ntb && ((v >> j) & 1)) lo |= 1u << S->tpos[j];
+      if (j + 4 < ntb && ((v >> j) & 1)) hi |= 1u << S->tpos[j + 4];
+    }
+    t[StageTab::UL + v] = lo;
+    t[StageTab::UH + v] = hi;
+    t[StageTab::SL + v] = swz(lo);
+    t[StageTab::SH + v] = swz(hi);
+  }
+}
+
+// Build the stage tables of pass P into `tabs` (every thread of the CTA calls
+// it; it ends with a block barrier).
+template <typename Real>
+__device__ __forceinline__ void build_pass_tabs(const PassRec& P, const StageRec* __restrict__ stages,
+                                                uint32_t* __restrict__ tabs) {
+  const int nst = P.stage_end - P.stage_begin;
+  for (int i = threadIdx.x; i < nst; i += blockDim.x)
+    build_stage_tab<Tr<Real>::kVecBit>(stages + P.stage_begin + i, tabs + i * kStageTabWords);
+  __syncthreads();
+}
+
 // Run stages [P.stage_begin, P.stage_end) of a pass on the tile held in shared
-// memory `sv` (swizzled vector slots).  Every thread of the CTA must call it
-// (it contains block barriers); threads >= nvec/16 only take part in them.
+// memory `sv` (swizzled vector slots), with the pass's stage tables in `tabs`.
+// Every thread of the CTA must call it (it contains block barriers); threads
+// >= nvec/16 only take part in them.
 template <typename Real>
 __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict__ sv, const PassRec& P,
-                                                const StageRec* __restrict__ stages,
+                                                const uint32_t* __restrict__ tabs,
                                                 const TileOp<Real>* __restrict__ ops, uint32_t ext) {
   using T = Tr<Real>;
   using C = typename T::C;
@@ -457,19 +548,16 @@ __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict
   constexpr int NRB = VB + kRegFree;
   const int tid = threadIdx.x;
   const uint32_t active_threads = (1u << (P.k - VB)) / kVecPerThread;
-  for (int s = P.stage_begin; s < P.stage_end; ++s) {
-    const StageRec* S = stages + s;
+  const int nst = P.stage_end - P.stage_begin;
+  for (int si = 0; si < nst; ++si) {
+    const uint32_t* Tb = tabs + si * kStageTabWords;
     if (uint32_t(tid) < active_threads) {
-      const int ntb = __ldg(&S->n_tbits);
-      uint32_t ub = 0;
-      for (int j = 0; j < ntb; ++j) ub |= ((uint32_t(tid) >> j) & 1u) << __ldg(&S->tpos[j]);
+      const uint32_t ub = Tb[StageTab::UL + (tid & 15)] | Tb[StageTab::UH + (tid >> 4)];
       // swz is linear over XOR and ub, vm_i have disjoint bits, so
       // swz(ub | sum vm_i) = swz(ub) ^ xor_i swz(vm_i).
-      const uint32_t s0 = swz(1u << (__ldg(&S->rpos[0]) - VB));
-      const uint32_t s1 = swz(1u << (__ldg(&S->rpos[1]) - VB));
-      const uint32_t s2 = swz(1u << (__ldg(&S->rpos[2]) - VB));
-      const uint32_t s3 = swz(1u << (__ldg(&S->rpos[3]) - VB));
-      const uint32_t sb = swz(ub);
+      const uint32_t sb = Tb[StageTab::SL + (tid & 15)] ^ Tb[StageTab::SH + (tid >> 4)];
+      const uint4 sq = *reinterpret_cast<const uint4*>(Tb + StageTab::S);
+      const uint32_t s0 = sq.x, s1 = sq.y, s2 = sq.z, s3 = sq.w;
       C a[NA];
 #pragma unroll
       for (int r = 0; r < kVecPerThread; ++r) {
@@ -478,34 +566,30 @@ __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict
         unpack_vec<Real>(sv[slot], a + r * APV);
       }
       const uint32_t vbase = (ub << VB) | ext;
-      apply_stage_ops<Real, NA, NRB>(a, ops, __ldg(&S->op_begin), __ldg(&S->op_end), vbase);
+      apply_stage_ops<Real, NA, NRB>(a, ops, int(Tb[StageTab::OB]), int(Tb[StageTab::OE]), vbase);
       // Write-back through the stage's deferred permutation pi(p) = A p ^ w:
       // register amplitude p goes to the slot of logical index pi(p).  Slot
       // offsets are linear in the free register bits (register bits
       // VB..VB+3); for complex64, bit 0 of pi(p) selects the 8-byte half.
-      auto regslot = [&](uint32_t m) -> uint32_t {
-        return (((m >> VB) & 1u) ? s0 : 0u) ^ (((m >> (VB + 1)) & 1u) ? s1 : 0u) ^
-               (((m >> (VB + 2)) & 1u) ? s2 : 0u) ^ (((m >> (VB + 3)) & 1u) ? s3 : 0u);
-      };
-      uint32_t w = uint32_t(__ldg(&S->sbx));
-      const int nc = __ldg(&S->ncond);
+      uint32_t wslot = Tb[StageTab::WS], hw = Tb[StageTab::WH];
+      const int nc = int(Tb[StageTab::NC]);
       for (int i = 0; i < nc; ++i) {
-        const uint32_t cm = __ldg(&S->cond_cnr[i]);
-        if ((vbase & cm) == cm) w ^= uint32_t(__ldg(&S->cond_w[i]));
+        const uint32_t cm = Tb[StageTab::CC + i];
+        if ((vbase & cm) == cm) {
+          wslot ^= Tb[StageTab::CS + i];
+          hw ^= Tb[StageTab::CH + i];
+        }
       }
-      const uint32_t m0 = uint32_t(__ldg(&S->scol[VB]));
-      const uint32_t m1 = uint32_t(__ldg(&S->scol[VB + 1]));
-      const uint32_t m2 = uint32_t(__ldg(&S->scol[VB + 2]));
-      const uint32_t m3 = uint32_t(__ldg(&S->scol[VB + 3]));
-      const uint32_t c0 = regslot(m0), c1 = regslot(m1), c2 = regslot(m2), c3 = regslot(m3);
-      const uint32_t sw = sb ^ regslot(w);
+      const uint4 cq = *reinterpret_cast<const uint4*>(Tb + StageTab::CW);
+      const uint32_t c0 = cq.x, c1 = cq.y, c2 = cq.z, c3 = cq.w;
+      const uint32_t sw = sb ^ wslot;
       if constexpr (VB == 1) {
-        const uint32_t mz = uint32_t(__ldg(&S->scol[0]));
+        const uint32_t mz = Tb[StageTab::MZ], hb = Tb[StageTab::HB];
+        const uint32_t h0 = hb & 1u, h1 = (hb >> 1) & 1u, h2 = (hb >> 2) & 1u, h3 = (hb >> 3) & 1u;
         if (mz == 1u) {
           // bit 0 stays bit 0: each vector keeps its pair, halves swap when
           // bit 0 of pi is flipped by the other register bits or by w
-          const uint32_t h0 = m0 & 1u, h1 = m1 & 1u, h2 = m2 & 1u, h3 = m3 & 1u, hw = w & 1u;
-          if ((h0 | h1 | h2 | h3 | hw) == 0u) {
+          if ((hb | hw) == 0u) {
             // no deferred flip of qubit 0 in this stage: whole vectors, no selects
 #pragma unroll
             for (int r = 0; r < kVecPerThread; ++r) {
@@ -526,8 +610,7 @@ __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict
           }
         } else {
           // bit 0 moves into other bits: store each amplitude separately
-          const uint32_t cz = regslot(mz), hz = mz & 1u;
-          const uint32_t h0 = m0 & 1u, h1 = m1 & 1u, h2 = m2 & 1u, h3 = m3 & 1u, hw = w & 1u;
+          const uint32_t cz = Tb[StageTab::CZ], hz = Tb[StageTab::HZ];
           C* sa = reinterpret_cast<C*>(sv);
 #pragma unroll
           for (int r = 0; r < kVecPerThread; ++r) {
@@ -550,7 +633,6 @@ __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict
     }
     __syncthreads();
   }
-
 }
 
 }  // namespace nqpu
