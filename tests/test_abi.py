@@ -103,5 +103,14 @@ def test_plan_stats_brickwork():
     assert 1 <= st["passes"] < 200
     pg = c.plan_stats(30, "c64", "pergate")
     assert pg["passes"] == 1780
-    st20 = c.plan_stats(30, "c128", "tiled")
-    assert st20["passes"] >= st["passes"]
+    # 64 KB complex64 tiles (13 qubits) need no more passes than 64 KB complex128 tiles (12)
+    lib = _lib.load()
+    old = lib.nqpu_tile_config_get(1)
+    assert lib.nqpu_tile_config_set(1, 2) == OK
+    try:
+        st13 = c.plan_stats(30, "c64", "tiled")
+    finally:
+        lib.nqpu_tile_config_set(1, old)
+    st12 = c.plan_stats(30, "c128", "tiled")
+    assert st12["passes"] >= st13["passes"]
+    assert lib.nqpu_tile_config_set(1, 3) == INVALID_PARAMETER
