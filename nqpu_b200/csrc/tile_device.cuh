@@ -117,6 +117,38 @@ __device__ __forceinline__ void rb_x1_generic(C (&a)[NA], int b, bool tc, uint32
   }
 }
 
+// X on register bit B, controlled by the register bits CM (compile time) and
+// by controls outside the registers (tc): per-thread selects (TC_ALWAYS would
+// make it a register renaming, which only straight-line code can afford).
+template <typename C, int NA, int B, int CM, bool TC_ALWAYS>
+__device__ __forceinline__ void rb_x1_fixed(C (&a)[NA], bool tc) {
+#pragma unroll
+  for (int i = 0; i < NA; ++i) {
+    if (i & (1 << B)) continue;
+    if ((i & CM) != CM) continue;
+    const int j = i | (1 << B);
+    const C x = a[i], y = a[j];
+    if constexpr (TC_ALWAYS) {
+      a[i] = y;
+      a[j] = x;
+    } else {
+      a[i] = csel(tc, y, x);
+      a[j] = csel(tc, x, y);
+    }
+  }
+}
+
+template <typename C, int NA, int NRB, int B, bool TC_ALWAYS>
+__device__ __forceinline__ void dispatch_x1_ctrl(C (&a)[NA], uint32_t creg, bool tc) {
+  switch (creg) {
+#define NQ_X1C(V) case (V == 0 ? 0 : (1 << (V - 1))): \
+    if constexpr (V == 0 || (V - 1 < NRB && V - 1 != B)) rb_x1_fixed<C, NA, B, (V == 0 ? 0 : (1 << (V - 1))), TC_ALWAYS>(a, tc); break;
+    NQ_X1C(0) NQ_X1C(1) NQ_X1C(2) NQ_X1C(3) NQ_X1C(4) NQ_X1C(5)
+#undef NQ_X1C
+    default: break;
+  }
+}
+
 // phase m on the register amplitudes whose bits CMASK are all set
 template <typename C, int NA, int CMASK>
 __device__ __forceinline__ void rb_ph(C (&a)[NA], C m, bool neg) {
@@ -332,11 +364,25 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
         break;
       }
       case OP_X1: {
-        // Only X1 ops the planner could not defer into the stage's write-back
-        // permutation reach the kernel (e.g. Toffoli).  They use selects, not
-        // register swaps: a register permutation at this join would make the
-        // allocator insert moves into every other op's path.
-        rb_x1_generic<C, NA>(a, int(rb0), tc, creg);
+        // X / CNOT kept in registers because later ops of the stage act on
+        // its qubits (the others are deferred into the write-back map).  At
+        // most one register control: a fixed register permutation; more
+        // (Toffoli): generic per-amplitude selects.
+        if (creg & (creg - 1)) {
+          rb_x1_generic<C, NA>(a, int(rb0), tc, creg);
+          break;
+        }
+        // selects even when tc is always true: a compile-time register
+        // permutation here would make the allocator shuffle (and spill) the
+        // register block on every other op's path
+        switch (rb0) {
+#define NQ_X1(B, _) case B: \
+          if constexpr (B < NRB) dispatch_x1_ctrl<C, NA, NRB, B, false>(a, creg, tc); \
+          break;
+          NQ_REG_CASES(NQ_X1, 0)
+#undef NQ_X1
+          default: break;
+        }
         break;
       }
       case OP_PH: {
