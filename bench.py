@@ -728,7 +728,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=64, help="batch form: plain-path sample size")
     ap.add_argument("--no-tune-cache", action="store_true")
     ap.add_argument("--requests", type=int, default=400, help="serve form: requests per offered rate")
-    ap.add_argument("--rates", default="20,40,80,160", help="serve form: offered rates (requests/s)")
+    ap.add_argument("--rates", default="20,40,80,160,320,640",
+                    help="serve form: offered rates (requests/s); the last one saturates the server")
     ap.add_argument("--lanes", type=int, default=16, help="serve form: concurrent requests on the device")
     ap.add_argument("--serve-budget-gb", type=float, default=64.0, help="serve form: HBM budget for states")
     ap.add_argument("--verbose", action="store_true")

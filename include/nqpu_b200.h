@@ -273,6 +273,19 @@ uint32_t     nqpu_tile_config_get(NqpuDtype dtype);
 NqpuError    nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_t num_qubits,
                                      NqpuDtype dtype, NqpuMode mode, uint64_t* out, uint32_t len);
 
+/* OpenQASM 2.0 (circuits/formats/qasm.rs:65 parse_qasm, :265 execute_qasm,
+ * :363 export): qreg/creg declarations, the qelib1.inc gate set, parameter
+ * expressions with pi, measure (terminal: results come from nqpu_sample /
+ * nqpu_measure_all), barrier.  NULL on a parse error (unknown gate, undeclared
+ * register, bad index, ...); *error_line (optional) gets its 1-based line. */
+NqpuCircuit* nqpu_circuit_from_qasm(const char* text, uint32_t* error_line);
+/* Qubit count of a circuit (0 on NULL). */
+uint32_t     nqpu_circuit_num_qubits(const NqpuCircuit* circuit);
+/* OpenQASM 2.0 text of the circuit into out (NUL-terminated, truncated to
+ * len-1 bytes); *needed = full length.  NQPU_INVALID_PARAMETER when a gate has
+ * no OpenQASM 2.0 form (custom matrices; written as a comment line). */
+NqpuError    nqpu_circuit_to_qasm(const NqpuCircuit* circuit, char* out, uint64_t len, uint64_t* needed);
+
 /* ------------------------------------------------------------------ */
 /* Batched execution (no counterpart in the reference): many circuits   */
 /* of different sizes in one persistent, graph-captured launch; each    */

@@ -279,6 +279,30 @@ class Circuit:
     def depth(self) -> int:
         return int(self.lib.nqpu_circuit_depth(self.h_))
 
+    @classmethod
+    def from_qasm(cls, text: str) -> "Circuit":
+        """Circuit from OpenQASM 2.0 text (nqpu_circuit_from_qasm)."""
+        lib = _lib.load()
+        line = C.c_uint32()
+        h = lib.nqpu_circuit_from_qasm(text.encode(), C.byref(line))
+        if not h:
+            raise ValueError(f"OpenQASM parse error at line {line.value}")
+        obj = cls.__new__(cls)
+        obj.lib = lib
+        obj.h_ = h
+        obj.num_qubits = int(lib.nqpu_circuit_num_qubits(h))
+        return obj
+
+    def to_qasm(self) -> str:
+        """OpenQASM 2.0 text of the circuit (nqpu_circuit_to_qasm)."""
+        need = C.c_uint64()
+        self.lib.nqpu_circuit_to_qasm(self.h_, None, 0, C.byref(need))
+        buf = C.create_string_buffer(int(need.value) + 1)
+        code = self.lib.nqpu_circuit_to_qasm(self.h_, buf, len(buf), C.byref(need))
+        if code not in (0, 2):
+            check(code, "circuit_to_qasm")
+        return buf.value.decode()
+
     def plan_stats(self, num_qubits: int, dtype: str = "c128", mode: str = "tiled"):
         out = (C.c_uint64 * 4)()
         check(self.lib.nqpu_circuit_plan_stats(self.h_, int(num_qubits), DTYPES[dtype], MODES[mode], out, 4),
