@@ -170,14 +170,12 @@ def traffic_from_profile(n, amp_bytes):
 
 def run_engine(args):
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from nqpu_b200 import replicas
+    rank, local, world = replicas.world()
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    replicas.init("nccl", timeout_s=300)
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
 
@@ -189,7 +187,11 @@ def run_engine(args):
     n, depth = args.qubits, args.depth
     if args.tile_ctas:
         _lib.check(lib.nqpu_tile_config_set(1 if args.dtype == "c64" else 0, args.tile_ctas), "tile_config")
-    gates = brickwork(n, depth, args.seed)
+    if args.circuit == "qft":
+        from nqpu_b200.circuits import qft
+        gates = qft(n)
+    else:
+        gates = brickwork(n, depth, args.seed)
     G = len(gates)
     amp_bytes = 8 if args.dtype == "c64" else 16
     S = (1 << n) * amp_bytes
@@ -221,8 +223,7 @@ def run_engine(args):
         pass
     clocks = ClockSampler(uuid)
     clocks.start()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize(dev)
     sv.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -236,16 +237,11 @@ def run_engine(args):
     ev1.synchronize()
     sv.synchronize()
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     clk = clocks.stop()
-    el_ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([el_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_ms = float(t.item())
-    total_gates = G * args.steps * world
-    value = total_gates / (el_ms / 1000.0)
+    # whole-job rate: every rank ran G * steps gates; time = max over ranks
+    value, el_s = replicas.replica_rate(G * args.steps, ev0.elapsed_time(ev1) / 1000.0, device=dev)
+    el_ms = el_s * 1000.0
     z_c64 = zout.copy()
 
     # roofline of the dominant kernel (the tiled pass): 2S algorithmic bytes per launch
@@ -309,11 +305,7 @@ def run_engine(args):
             _lib.check(lib.nqpu_expectation_z_all(sv.h_, zptr, n), "zall")
             t_e2e.append(time.perf_counter() - t0)
             c2.close()
-        et = float(np.mean(t_e2e))
-        if world > 1:
-            t = torch.tensor([et], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            et = float(t.item())
+        et = replicas.max_over_ranks(float(np.mean(t_e2e)), device=dev)
         e2e = {"value": G * world / et, "unit": "gates/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 8 * n, "seconds_per_step": et,
                "timing": "host wall clock around create+execute+reduce (includes plan build)"}
@@ -326,11 +318,13 @@ def run_engine(args):
 
     if rank == 0:
         line = {
-            "metric": "gates/s (30q complex64 brickwork, unfused)", "value": value, "unit": "gates/s",
+            "metric": ("gates/s (30q complex64 brickwork, unfused)" if args.circuit == "brickwork"
+                       else f"gates/s ({n}q QFT, unfused)"), "value": value, "unit": "gates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
-            "config": {"workload": f"brickwork {n}q depth {depth} {'complex64' if args.dtype == 'c64' else 'complex128'}",
+            "config": {"workload": (f"brickwork {n}q depth {depth}" if args.circuit == "brickwork" else f"QFT {n}q")
+                                   + f" {'complex64' if args.dtype == 'c64' else 'complex128'}",
                        "gates": G, "seed": args.seed, "engine_mode": args.mode,
                        "plan": {"passes": stats["passes"], "stages": stats["stages"]},
                        "tile_ctas_per_sm": int(lib.nqpu_tile_config_get(1 if args.dtype == "c64" else 0)),
@@ -342,9 +336,7 @@ def run_engine(args):
         print(json.dumps(line), flush=True)
     sv.close()
     circ.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.shutdown()
 
 
 def run_precision(args):
@@ -709,6 +701,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=40)
+    ap.add_argument("--circuit", default="brickwork", choices=["brickwork", "qft"],
+                    help="plain form circuit: random brickwork (headline) or the QFT")
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
     ap.add_argument("--mode", default="tiled", choices=["tiled", "pergate", "fused"])
     ap.add_argument("--seed", type=int, default=1)

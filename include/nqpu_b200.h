@@ -255,6 +255,19 @@ NqpuError   nqpu_expectation_z_all_noalloc(const void* d_amplitudes, uint32_t nu
 NqpuCircuit* nqpu_circuit_create_ex(uint32_t num_qubits);
 /* Run with an explicit engine mode. */
 NqpuError    nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode);
+/* Mid-circuit measurement (QuantumSimulator::measure_qubit, lib.rs:1835) and
+ * OpenQASM reset: the circuit runs as segments between them; a measurement
+ * collapses the state with the next draw of the thread-local RNG (as
+ * nqpu_measure); a reset measures the same way and flips the qubit back to |0>
+ * when it came out 1 (unlike nqpu_gate_reset_qubit, which keeps the reference's
+ * projection, GateOperations::reset_qubit lib.rs:1705).  Batches and the
+ * request server take measurement-free circuits. */
+NqpuError    nqpu_circuit_add_measure(NqpuCircuit* c, uint32_t q);
+NqpuError    nqpu_circuit_add_reset(NqpuCircuit* c, uint32_t q);
+/* Execute and return the outcomes of the circuit's measurements in order
+ * (*count of them; len must hold every measurement of the circuit). */
+NqpuError    nqpu_circuit_execute_measured(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,
+                                           uint32_t* outcomes, uint32_t len, uint32_t* count);
 /* Run the circuit recording a CUDA event between consecutive kernel launches;
  * launch_ms[i] = device time of launch i (i < *count <= len). */
 NqpuError    nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,

@@ -13,6 +13,7 @@ per generator) stand in for the configurations the engine is measured on:
     open chain: RZZ(2 J dt) on every bond then RX(2 h_i dt) on every site.
   * `hea`: hardware-efficient ansatz, RY(theta) RZ(phi) on all qubits + CZ ladder.
   * `serving_mix`: Poisson arrivals of brickwork requests of log-uniform size.
+  * `qft`: the quantum Fourier transform (H + controlled-phase chains + SWAPs).
 """
 from __future__ import annotations
 
@@ -25,12 +26,15 @@ GATE_CODES = {
     "h": 0, "x": 1, "y": 2, "z": 3, "s": 4, "t": 5, "sx": 6, "rx": 7, "ry": 8, "rz": 9, "p": 10,
     "u3": 11, "cx": 12, "cz": 13, "swap": 14, "iswap": 15, "cp": 16, "crx": 17, "cry": 18,
     "crz": 19, "rzz": 20, "rxx": 21, "ryy": 22, "ccx": 23, "ccz": 24, "cswap": 25,
-    "custom1": 26, "custom2": 27, "u2lo": 28, "cu": 29,
+    "custom1": 26, "custom2": 27, "u2lo": 28, "cu": 29, "measure": 30, "reset": 31,
 }
+# Mid-circuit measurement and reset (circuit-level, one qubit, no parameters);
+# ARITY covers the unitary gates only.
+MID_GATES = ("measure", "reset")
 ARITY = {name: (3 if name in ("ccx", "ccz", "cswap") else
                 2 if name in ("cx", "cz", "swap", "iswap", "cp", "crx", "cry", "crz", "rzz", "rxx",
                               "ryy", "custom2", "u2lo", "cu") else 1)
-         for name in GATE_CODES}
+         for name in GATE_CODES if name not in MID_GATES}
 
 NPARAMS = {name: 0 for name in GATE_CODES}
 NPARAMS.update({"rx": 1, "ry": 1, "rz": 1, "p": 1, "u3": 3, "cp": 1, "crx": 1, "cry": 1, "crz": 1,
@@ -116,6 +120,20 @@ def tfim_trotter(n: int, steps: int, seed: int, J: float = 1.0, dt: float = 0.05
     for i in range(n):
         step.append(("rx", (i,), (2.0 * float(h[i]) * dt,)))
     return step * steps, h
+
+
+def qft(n: int):
+    """Quantum Fourier transform (no input state preparation): for i = n-1..0,
+    H(i) then controlled phases CP(pi / 2^(i-j)) from qubit j < i onto i, then
+    the qubit-order reversal by n/2 SWAPs.  n(n+1)/2 + n/2 gates."""
+    gates = []
+    for i in range(n - 1, -1, -1):
+        gates.append(("h", (i,), ()))
+        for j in range(i - 1, -1, -1):
+            gates.append(("cp", (j, i), (math.pi / 2 ** (i - j),)))
+    for i in range(n // 2):
+        gates.append(("swap", (i, n - 1 - i), ()))
+    return gates
 
 
 def neel_index(n: int) -> int:

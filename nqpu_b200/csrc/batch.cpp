@@ -242,6 +242,7 @@ extern "C" NqpuError nqpu_batch_add_ising(NqpuBatch* batch, const NqpuCircuit* c
   if (!batch || !circuit || !h) return NQPU_NULL_POINTER;
   const CircuitImpl* c = reinterpret_cast<const CircuitImpl*>(circuit);
   if (c->n < 5 || c->n > 24) return NQPU_INVALID_PARAMETER;  // batched circuits: 5..24 qubits (3 bond tables)
+  if (circuit_has_mid(c->gates)) return NQPU_INVALID_PARAMETER;  // measurement-free circuits only
   if (c->n > 1 && !J) return NQPU_NULL_POINTER;
   BatchImpl* b = B(batch);
   BatchEntry e;

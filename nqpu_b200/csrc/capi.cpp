@@ -332,11 +332,7 @@ extern "C" NqpuError nqpu_gate_reset_qubit(NqpuState* state, uint32_t qubit) {
   if (!state) return NQPU_NULL_POINTER;
   StateImpl* s = S(state);
   if (qubit >= s->n) return NQPU_INVALID_QUBIT;
-  std::vector<double> z(s->n + 1);
-  NQ_TRY(state_zsums(s, z.data(), nullptr));
-  const double keep = z[0] - z[1 + qubit];  // norm of the |0> half
-  const double f = keep > 0.0 ? 1.0 / std::sqrt(keep) : 1.0;
-  NQ_TRY(launch_collapse(s->dt, s->amp, int(s->n), int(qubit), 0, f, s->stream, device_sms()));
+  NQ_TRY(state_reset_qubit(s, qubit));
   return NQPU_OK;
 }
 
@@ -344,15 +340,9 @@ extern "C" NqpuError nqpu_gate_reset_qubit(NqpuState* state, uint32_t qubit) {
 // Measurement and reductions
 // ---------------------------------------------------------------------------
 static NqpuError measure_one(StateImpl* s, uint32_t qubit, NqpuMeasurement* out) {
-  std::vector<double> z(s->n + 1);
-  NQ_TRY(state_zsums(s, z.data(), nullptr));
-  const double prob0 = z[0] - z[1 + qubit];  // sum over bit q == 0
-  const double prob1 = 1.0 - prob0;          // c_ffi.rs:546
-  const double r = next_random_f64();
-  const uint32_t outcome = r < prob0 ? 0u : 1u;
-  const double po = outcome == 0 ? prob0 : prob1;
-  const double renorm = 1.0 / std::sqrt(po);
-  NQ_TRY(launch_collapse(s->dt, s->amp, int(s->n), int(qubit), int(outcome), renorm, s->stream, device_sms()));
+  uint32_t outcome = 0;
+  double po = 0.0;
+  NQ_TRY(state_measure(s, qubit, &outcome, &po));
   out->outcome = outcome;
   out->probability = po;
   return NQPU_OK;
@@ -549,6 +539,8 @@ NQ_CADD1(nqpu_circuit_add_y, G_Y)
 NQ_CADD1(nqpu_circuit_add_z, G_Z)
 NQ_CADD1(nqpu_circuit_add_s, G_S)
 NQ_CADD1(nqpu_circuit_add_t, G_T)
+NQ_CADD1(nqpu_circuit_add_measure, G_MEASURE)
+NQ_CADD1(nqpu_circuit_add_reset, G_RESET)
 NQ_CADD1(nqpu_circuit_add_sx, G_SX)
 NQ_CADD1P(nqpu_circuit_add_rx, G_RX)
 NQ_CADD1P(nqpu_circuit_add_ry, G_RY)
@@ -605,6 +597,27 @@ extern "C" NqpuError nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuSta
   cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode));
   if (e != cudaSuccess) return map_cuda(e);
   NQ_TRY(cudaStreamSynchronize(s->stream));
+  return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_circuit_execute_measured(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode,
+                                                   uint32_t* outcomes, uint32_t len, uint32_t* count) {
+  if (!circuit || !state || !count) return NQPU_NULL_POINTER;
+  const CircuitImpl* c = Cc(circuit);
+  StateImpl* s = S(state);
+  if (c->n > s->n) return NQPU_INVALID_PARAMETER;
+  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED)
+    return NQPU_INVALID_PARAMETER;
+  if (mode == NQPU_MODE_FUSED && (s->dt != DType::C64 || s->n < 12)) return NQPU_INVALID_PARAMETER;
+  uint32_t nmeas = 0;
+  for (const GateRec& g : c->gates) nmeas += g.code == G_MEASURE ? 1u : 0u;
+  if (nmeas > 0 && (!outcomes || len < nmeas)) return NQPU_INVALID_PARAMETER;
+  std::vector<uint32_t> out;
+  cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode), nullptr, &out);
+  if (e != cudaSuccess) return map_cuda(e);
+  NQ_TRY(cudaStreamSynchronize(s->stream));
+  for (size_t i = 0; i < out.size(); ++i) outcomes[i] = out[i];
+  *count = uint32_t(out.size());
   return NQPU_OK;
 }
 

@@ -92,6 +92,32 @@ cudaError_t state_zsums(const StateImpl* s, double* zs, double* total) {
   return cudaSuccess;
 }
 
+cudaError_t state_measure(StateImpl* s, uint32_t qubit, uint32_t* outcome, double* probability) {
+  std::vector<double> z(s->n + 1);
+  cudaError_t e = state_zsums(s, z.data(), nullptr);
+  if (e != cudaSuccess) return e;
+  const double prob0 = z[0] - z[1 + qubit];  // sum over bit q == 0
+  const double prob1 = 1.0 - prob0;          // c_ffi.rs:546
+  const double r = next_random_f64();
+  const uint32_t out = r < prob0 ? 0u : 1u;
+  const double po = out == 0 ? prob0 : prob1;
+  const double renorm = 1.0 / std::sqrt(po);
+  e = launch_collapse(s->dt, s->amp, int(s->n), int(qubit), int(out), renorm, s->stream, device_sms());
+  if (e != cudaSuccess) return e;
+  *outcome = out;
+  if (probability) *probability = po;
+  return cudaSuccess;
+}
+
+cudaError_t state_reset_qubit(StateImpl* s, uint32_t qubit) {
+  std::vector<double> z(s->n + 1);
+  cudaError_t e = state_zsums(s, z.data(), nullptr);
+  if (e != cudaSuccess) return e;
+  const double keep = z[0] - z[1 + qubit];  // norm of the |0> half
+  const double f = keep > 0.0 ? 1.0 / std::sqrt(keep) : 1.0;
+  return launch_collapse(s->dt, s->amp, int(s->n), int(qubit), 0, f, s->stream, device_sms());
+}
+
 cudaError_t state_pauli(const StateImpl* s, uint64_t xm, uint64_t zm, uint64_t ym, double* out2) {
   cudaError_t e = launch_pauli(s->dt, s->amp, int(s->n), xm, zm, ym, s->scratch, s->d_small, s->stream, device_sms());
   if (e != cudaSuccess) return e;
@@ -219,8 +245,26 @@ void circuit_free(CircuitImpl* c) {
   delete c;
 }
 
-static bool plan_host(const CircuitImpl* c, uint32_t n, DType dt, int mode, DevicePlan* p) {
-  p->ops = lower_circuit(c->gates);
+bool circuit_has_mid(const std::vector<GateRec>& gates) {
+  for (const GateRec& g : gates)
+    if (gate_is_mid(g.code)) return true;
+  return false;
+}
+
+std::vector<Segment> circuit_segments(const std::vector<GateRec>& gates) {
+  std::vector<Segment> segs;
+  size_t b = 0;
+  for (size_t i = 0; i < gates.size(); ++i)
+    if (gate_is_mid(gates[i].code)) {
+      segs.push_back(Segment{b, i, long(i)});
+      b = i + 1;
+    }
+  segs.push_back(Segment{b, gates.size(), -1});
+  return segs;
+}
+
+static bool plan_host(const CircuitImpl* c, const Segment& seg, uint32_t n, DType dt, int mode, DevicePlan* p) {
+  p->ops = lower_circuit(std::vector<GateRec>(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end)));
   p->stats = PlanStats{};
   if (mode == NQPU_MODE_TILED && int(n) >= tile_min_qubits(dt)) {
     std::string err;
@@ -238,14 +282,22 @@ static bool plan_host(const CircuitImpl* c, uint32_t n, DType dt, int mode, Devi
 }
 
 bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out) {
-  DevicePlan p;
-  if (mode == NQPU_MODE_FUSED) {
-    p.ops = lower_circuit(c->gates);
-    bool ok = fused_plan_stats(p.ops, int(n), dt, out);
-    return ok;
+  *out = PlanStats{};
+  for (const Segment& seg : circuit_segments(c->gates)) {
+    DevicePlan p;
+    PlanStats st;
+    if (mode == NQPU_MODE_FUSED) {
+      p.ops = lower_circuit(std::vector<GateRec>(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end)));
+      if (!fused_plan_stats(p.ops, int(n), dt, &st)) return false;
+    } else {
+      if (!plan_host(c, seg, n, dt, mode, &p)) return false;
+      st = p.stats;
+    }
+    out->passes += st.passes;
+    out->ops += st.ops;
+    out->stages += st.stages;
+    out->upload_bytes += st.upload_bytes;
   }
-  if (!plan_host(c, n, dt, mode, &p)) return false;
-  *out = p.stats;
   return true;
 }
 
@@ -285,10 +337,45 @@ static cudaError_t mark(std::vector<cudaEvent_t>* ev, cudaStream_t st) {
   return cudaEventRecord(e, st);
 }
 
-cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cudaEvent_t>* events) {
+static cudaError_t segment_run(CircuitImpl* c, const Segment& seg, int si, StateImpl* s, int mode,
+                               std::vector<cudaEvent_t>* events);
+
+cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cudaEvent_t>* events,
+                        std::vector<uint32_t>* outcomes) {
   std::lock_guard<std::mutex> lk(c->mu);
+  const std::vector<Segment> segs = circuit_segments(c->gates);
+  for (size_t si = 0; si < segs.size(); ++si) {
+    const Segment& seg = segs[si];
+    cudaError_t e = segment_run(c, seg, int(si), s, mode, events);
+    if (e != cudaSuccess) return e;
+    if (seg.mid < 0) break;
+    const GateRec& g = c->gates[size_t(seg.mid)];
+    if (g.code == G_MEASURE) {
+      uint32_t out = 0;
+      if ((e = state_measure(s, uint32_t(g.q[0]), &out, nullptr)) != cudaSuccess) return e;
+      if (outcomes) outcomes->push_back(out);
+    } else {
+      // OpenQASM reset: measure (one RNG draw) and flip the qubit back to |0>
+      // when it came out 1 (the state API's nqpu_gate_reset_qubit keeps the
+      // reference's projection, GateOperations::reset_qubit)
+      uint32_t out = 0;
+      if ((e = state_measure(s, uint32_t(g.q[0]), &out, nullptr)) != cudaSuccess) return e;
+      if (out == 1) {
+        Op x;
+        x.kind = OP_X1;
+        x.t0 = int8_t(g.q[0]);
+        if ((e = launch_pergate(s->dt, s->amp, int(s->n), x, s->stream, device_sms())) != cudaSuccess) return e;
+      }
+    }
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t segment_run(CircuitImpl* c, const Segment& seg, int si, StateImpl* s, int mode,
+                               std::vector<cudaEvent_t>* events) {
+  if (seg.begin == seg.end) return cudaSuccess;
   const int effective = (mode == NQPU_MODE_TILED && int(s->n) < tile_min_qubits(s->dt)) ? int(NQPU_MODE_PERGATE) : mode;
-  const auto key = std::make_tuple(s->n, int(s->dt), effective);
+  const auto key = std::make_tuple(s->n, int(s->dt), effective, si);
   DevicePlan*& p = c->plans[key];
   // rebuild when the circuit changed or the tiled kernel's tile size did
   if (p && (p->version != c->version || (effective == NQPU_MODE_TILED && p->kmax != tile_kmax_for(s->dt)))) {
@@ -298,7 +385,7 @@ cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cuda
   }
   if (!p) {
     p = new DevicePlan();
-    if (!plan_host(c, s->n, s->dt, effective, p)) {
+    if (!plan_host(c, seg, s->n, s->dt, effective, p)) {
       plan_free(p);
       p = nullptr;
       return cudaErrorInvalidValue;

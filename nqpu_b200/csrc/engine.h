@@ -61,15 +61,33 @@ struct CircuitImpl {
   uint32_t n = 0;
   std::vector<GateRec> gates;
   uint64_t version = 0;
-  std::map<std::tuple<uint32_t, int, int>, DevicePlan*> plans;
+  // cached plans per (state qubits, dtype, mode, segment); segments are the
+  // gate runs between mid-circuit measurements / resets
+  std::map<std::tuple<uint32_t, int, int, int>, DevicePlan*> plans;
   std::mutex mu;
 };
+
+// Gate runs of a circuit between mid-circuit measure / reset gates:
+// [begin, end) ranges of c->gates, with the mid gate that follows (index, or
+// -1 after the last run).
+struct Segment {
+  size_t begin, end;
+  long mid;
+};
+std::vector<Segment> circuit_segments(const std::vector<GateRec>& gates);
+bool circuit_has_mid(const std::vector<GateRec>& gates);
+
+// Measure one qubit (collapse with the thread-local RNG draw, c_ffi.rs:537-560
+// rule) / project it onto |0> and renormalise (lib.rs:1705).
+cudaError_t state_measure(StateImpl* s, uint32_t qubit, uint32_t* outcome, double* probability);
+cudaError_t state_reset_qubit(StateImpl* s, uint32_t qubit);
 
 void circuit_free(CircuitImpl* c);
 // Queue the circuit on the state's stream (no host sync).  With `events`, an
 // event is recorded before the first launch and after every launch.
 cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode,
-                        std::vector<cudaEvent_t>* events = nullptr);
+                        std::vector<cudaEvent_t>* events = nullptr,
+                        std::vector<uint32_t>* outcomes = nullptr);
 bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out);
 
 // Run a lowered op list on a state with the given mode (used by batch/server).

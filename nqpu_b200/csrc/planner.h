@@ -14,8 +14,13 @@ enum GateCode : uint8_t {
   G_CX, G_CZ, G_SWAP, G_ISWAP, G_CP, G_CRX, G_CRY, G_CRZ,
   G_RZZ, G_RXX, G_RYY, G_CCX, G_CCZ, G_CSWAP,
   G_CUSTOM1, G_CUSTOM2_FFI, G_U2_LO, G_CU,
+  // mid-circuit measurement (QuantumSimulator::measure_qubit, lib.rs:1835)
+  // and OpenQASM reset (measure, then X when the outcome is 1): not lowered to
+  // ops, they split a circuit into segments that run as separate plans
+  G_MEASURE, G_RESET,
   G_COUNT
 };
+inline bool gate_is_mid(uint8_t code) { return code == G_MEASURE || code == G_RESET; }
 
 struct GateRec {
   uint8_t code = G_H;

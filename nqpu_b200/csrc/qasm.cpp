@@ -13,9 +13,11 @@
 //   * a single-qubit gate applied to a whole register acts on every qubit of
 //     it, two-qubit gates on two registers act pairwise;
 //   * statements may span lines and several may share a line.
-// Measurements end the circuit in this engine (results come from
-// nqpu_sample / nqpu_measure_all on the final state); they are accepted and
-// recorded only as the set of measured qubits.  `barrier` and `id` are no-ops.
+// `measure` becomes a measurement gate per qubit and `reset` a reset gate
+// (mid-circuit: nqpu_circuit_execute_measured returns the outcomes in order,
+// as the reference's execute_qasm collects measure_qubit results,
+// qasm.rs:270-276); the classical bit a measurement writes is not tracked.
+// `barrier` and `id` are no-ops.
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -317,10 +319,20 @@ struct Parser {
       pos += 2;
       if (!qarg(&c, true) || !expect(';')) return false;
       if (q.size() != c.size()) return fail("measure: register sizes differ");
-      for (int x : q) measured.push_back(x);
+      for (int x : q) {
+        measured.push_back(x);
+        if (!add(G_MEASURE, std::vector<int>{x})) return false;
+      }
       return true;
     }
-    if (kw == "reset" || kw == "gate" || kw == "opaque" || kw == "if")
+    if (kw == "reset") {
+      std::vector<int> q;
+      if (!qarg(&q) || !expect(';')) return false;
+      for (int x : q)
+        if (!add(G_RESET, std::vector<int>{x})) return false;
+      return true;
+    }
+    if (kw == "gate" || kw == "opaque" || kw == "if")
       return fail("'" + kw + "' is not supported");
     // gate application
     std::vector<double> params;
@@ -407,6 +419,8 @@ bool gate_qasm(const GateRec& g, std::ostringstream& o) {
       o << "cu(" << f(g.p[0]) << "," << f(g.p[1]) << "," << f(g.p[2]) << "," << f(g.p[3]) << ") " << q(0) << ","
         << q(1);
       break;
+    case G_MEASURE: o << "measure " << q(0) << " -> c[" << g.q[0] << "]"; break;
+    case G_RESET: o << "reset " << q(0); break;
     default:
       o << "// gate code " << int(g.code) << " (custom matrix) has no OpenQASM 2.0 form";
       return false;
@@ -447,6 +461,7 @@ extern "C" NqpuError nqpu_circuit_to_qasm(const NqpuCircuit* circuit, char* out,
   const CircuitImpl* c = reinterpret_cast<const CircuitImpl*>(circuit);
   std::ostringstream o;
   o << "OPENQASM 2.0;\ninclude \"qelib1.inc\";\nqreg q[" << c->n << "];\n";
+  if (circuit_has_mid(c->gates)) o << "creg c[" << c->n << "];\n";
   bool all = true;
   for (const GateRec& g : c->gates) {
     all = gate_qasm(g, o) && all;

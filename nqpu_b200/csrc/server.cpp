@@ -437,6 +437,7 @@ extern "C" NqpuError nqpu_server_submit(NqpuServer* server, const NqpuCircuit* c
   const double t0 = now_s();
   const CircuitImpl* c = reinterpret_cast<const CircuitImpl*>(circuit);
   if (c->n == 0 || c->n > sv->cfg.max_qubits) return NQPU_INVALID_PARAMETER;
+  if (circuit_has_mid(c->gates)) return NQPU_INVALID_PARAMETER;  // measurement-free circuits only
   if (kind != NQPU_REQUEST_ZALL && kind != NQPU_REQUEST_SHOTS) return NQPU_INVALID_PARAMETER;
   if (kind == NQPU_REQUEST_SHOTS && (shots == 0 || shots > sv->cfg.max_shots)) return NQPU_INVALID_PARAMETER;
   auto r = std::make_shared<Request>();

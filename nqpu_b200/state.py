@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import NqpuComplex, NqpuMeasurement, check
-from .circuits import ARITY, NPARAMS
+from .circuits import ARITY, MID_GATES, NPARAMS
 
 C128, C64 = 0, 1
 MODES = {"tiled": 0, "pergate": 1, "fused": 2}
@@ -50,6 +50,7 @@ _CIRC_FN = {
     "cry": "nqpu_circuit_add_cry", "crz": "nqpu_circuit_add_crz", "rzz": "nqpu_circuit_add_rzz",
     "rxx": "nqpu_circuit_add_rxx", "ryy": "nqpu_circuit_add_ryy", "ccx": "nqpu_circuit_add_toffoli",
     "ccz": "nqpu_circuit_add_ccz", "cswap": "nqpu_circuit_add_cswap", "cu": "nqpu_circuit_add_cu",
+    "measure": "nqpu_circuit_add_measure", "reset": "nqpu_circuit_add_reset",
 }
 
 
@@ -252,6 +253,10 @@ class Circuit:
 
     def add(self, name: str, qubits, params=(), matrix=None):
         qs = [int(q) for q in qubits]
+        if name in MID_GATES:
+            if len(qs) != 1:
+                raise ValueError(f"{name} takes 1 qubit")
+            return check(getattr(self.lib, _CIRC_FN[name])(self.h_, qs[0]), name)
         if len(qs) != ARITY[name]:
             raise ValueError(f"{name} takes {ARITY[name]} qubits")
         if name == "custom1":
@@ -270,6 +275,15 @@ class Circuit:
 
     def execute(self, state: StateVector, mode: str = "tiled"):
         check(self.lib.nqpu_circuit_execute_ex(self.h_, state.h_, MODES[mode]), "circuit_execute")
+
+    def execute_measured(self, state: StateVector, mode: str = "tiled") -> np.ndarray:
+        """Execute and return the outcomes of the mid-circuit measurements in order."""
+        nmeas = 64 + self.gate_count
+        out = (C.c_uint32 * nmeas)()
+        cnt = C.c_uint32()
+        check(self.lib.nqpu_circuit_execute_measured(self.h_, state.h_, MODES[mode], out, nmeas, C.byref(cnt)),
+              "circuit_execute_measured")
+        return np.array(out[:cnt.value], dtype=np.uint32)
 
     @property
     def gate_count(self) -> int:

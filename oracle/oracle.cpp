@@ -315,8 +315,34 @@ void op_reset_qubit(State<R>& s, int q) {  // lib.rs:1705
 // ---- gate dispatch (apply_gate_to_state, ascii_viz.rs:124) -----------------
 enum Code {
   H, X, Y, Z, S, T, SX, RX, RY, RZ, P, U3, CX, CZ, SWAP, ISWAP, CP, CRX, CRY, CRZ, RZZ, RXX, RYY,
-  CCX, CCZ, CSWAP, CUSTOM1, CUSTOM2, U2LO, CU
+  CCX, CCZ, CSWAP, CUSTOM1, CUSTOM2, U2LO, CU, MEASURE, RESET
 };
+
+}  // namespace
+extern "C" double oracle_next_random();  // xorshift64* draw (c_ffi.rs:56-66)
+namespace {
+std::vector<uint32_t> g_outcomes;      // outcomes of MEASURE gates, in order
+
+// Mid-circuit measurement (QuantumSimulator::measure_qubit, lib.rs:1835, with
+// the C FFI's probability rule, c_ffi.rs:537-560): P(0) summed over the |0>
+// half, outcome 0 iff r < P(0), the other half zeroed and the kept half scaled
+// by 1/sqrt(P(outcome)).
+template <typename R>
+void op_measure(State<R>& s, int q) {
+  const uint64_t mask = 1ull << q;
+  double p0 = 0.0;
+  for (uint64_t i = 0; i < s.dim(); ++i)
+    if (!(i & mask)) p0 += double(s.a[i].re) * s.a[i].re + double(s.a[i].im) * s.a[i].im;
+  const double r = oracle_next_random();
+  const uint32_t out = r < p0 ? 0u : 1u;
+  const double po = out == 0 ? p0 : 1.0 - p0;
+  const R f = R(1.0 / std::sqrt(po));
+  for (uint64_t i = 0; i < s.dim(); ++i) {
+    if (((i & mask) != 0) != (out == 1)) s.a[i] = {R(0), R(0)};
+    else { s.a[i].re *= f; s.a[i].im *= f; }
+  }
+  g_outcomes.push_back(out);
+}
 
 template <typename R>
 void apply_flat(State<R>& s, const double* g) {
@@ -325,6 +351,15 @@ void apply_flat(State<R>& s, const double* g) {
   const double th = g[4], ph = g[5], la = g[6], ga = g[7];
   auto M = [&](int i) { return Cx<R>{R(g[8 + 2 * i]), R(g[9 + 2 * i])}; };
   switch (code) {
+    case MEASURE: op_measure(s, a); break;
+    case RESET: {  // OpenQASM reset: measure (not recorded), flip back to |0> on 1
+      const size_t k = g_outcomes.size();
+      op_measure(s, a);
+      const uint32_t out = g_outcomes.back();
+      g_outcomes.resize(k);
+      if (out == 1) op_x(s, a);
+      break;
+    }
     case H: op_h(s, a); break;
     case X: op_x(s, a); break;
     case Y: op_y(s, a); break;
@@ -651,6 +686,14 @@ void oracle_sample_uniforms(void* h, const double* u, int shots, uint64_t* out) 
     }
     return 0;
   });
+}
+
+// outcomes of the MEASURE gates applied since the last call (up to max)
+int oracle_take_outcomes(uint32_t* out, int max) {
+  const int k = int(std::min<size_t>(g_outcomes.size(), size_t(max)));
+  for (int i = 0; i < k; ++i) out[i] = g_outcomes[size_t(i)];
+  g_outcomes.clear();
+  return k;
 }
 
 // xorshift64* of c_ffi.rs:56-66 and nqpu_set_seed (c_ffi.rs:1444)

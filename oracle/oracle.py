@@ -40,6 +40,7 @@ def lib():
             "oracle_probabilities": (None, [vp, pd]),
             "oracle_sample_uniforms": (None, [vp, pd, i, C.POINTER(C.c_uint64)]),
             "oracle_set_seed": (None, [u64]), "oracle_next_random": (d, []),
+            "oracle_take_outcomes": (C.c_int, [C.POINTER(C.c_uint32), C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -77,6 +78,13 @@ class OracleState:
     def set_amplitudes(self, arr):
         a = np.ascontiguousarray(np.asarray(arr, dtype=np.complex128)).view(np.float64)
         self.L.oracle_state_set(self.h, a.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def take_outcomes(self, max_count: int = 4096) -> np.ndarray:
+        """Outcomes of the 'measure' gates applied since the last call (xorshift64*
+        draws from the seed set by set_seed)."""
+        out = (C.c_uint32 * max_count)()
+        k = self.L.oracle_take_outcomes(out, max_count)
+        return np.array(out[:k], dtype=np.uint32)
 
     def reset_qubit(self, q):
         self.L.oracle_reset_qubit(self.h, q)
@@ -119,6 +127,11 @@ def xorshift_uniforms(seed: int, count: int) -> np.ndarray:
     L = lib()
     L.oracle_set_seed(seed)
     return np.array([L.oracle_next_random() for _ in range(count)])
+
+
+def set_seed(seed: int):
+    """Seed the oracle's xorshift64* stream (the draws its 'measure' gates use)."""
+    lib().oracle_set_seed(int(seed))
 
 
 def set_threads(t: int):

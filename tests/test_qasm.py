@@ -28,10 +28,10 @@ measure q -> c;
 def test_reference_import_example():
     c = Circuit.from_qasm(BELL)
     assert c.num_qubits == 2
-    # the reference counts the two measurements as gates (qasm.rs:556); here
-    # measurements are terminal and read from the final state
-    assert c.gate_count == 2
-    assert "h q[0];" in c.to_qasm() and "cx q[0],q[1];" in c.to_qasm()
+    assert c.gate_count == 4  # h, cx, measure q[0], measure q[1] (qasm.rs:556)
+    out = c.to_qasm()
+    assert "h q[0];" in out and "cx q[0],q[1];" in out
+    assert "creg c[2];" in out and "measure q[1] -> c[1];" in out
 
 
 def test_gate_set_expressions_and_broadcast():
@@ -56,8 +56,8 @@ measure a[0] -> m[0];
 """
     c = Circuit.from_qasm(text)
     assert c.num_qubits == 4
-    # 3 + 4 + 3 + 4 + 4 + 5 + 3 + 2 (h a) + 2 (cx a, b pairwise)
-    assert c.gate_count == 30
+    # 3 + 4 + 3 + 4 + 4 + 5 + 3 + 2 (h a) + 2 (cx a, b pairwise) + 1 measure
+    assert c.gate_count == 31
     out = c.to_qasm()
     assert "u3(1.5707963267948966,-0.78539816339744828,2.0943951023931953) q[0];" in out
     assert "u3(1.5707963267948966,0,3.1415926535897931) q[1];" in out  # u2(phi, lambda)
@@ -75,7 +75,7 @@ measure a[0] -> m[0];
     ("qreg q[2];\ncx q[0],q[0];\n", 2),
     ("qreg q[2];\n\nrx(pi/0) q[0];\n", 3),
     ("qreg q[2];\nrx(theta) q[0];\n", 2),
-    ("qreg q[2];\nreset q[0];\n", 2),
+    ("qreg q[2];\ngate foo a { h a; }\n", 2),
     ("qreg q[2];\nh q[0]\n", 3),
 ])
 def test_errors_report_line(bad, line):
