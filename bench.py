@@ -530,7 +530,7 @@ def run_batch(args):
             c.close()
 
     line = {
-        "form": "batch", "metric": "circuits/s (4096 mixed-size HEA circuits, <H> per circuit)",
+        "form": "batch", "metric": f"circuits/s ({count} mixed-size HEA circuits, <H> per circuit)",
         "value": value, "unit": "circuits/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
         "ms_per_step": tot_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c64", "data": "synthetic",
