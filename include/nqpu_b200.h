@@ -255,6 +255,19 @@ NqpuError   nqpu_expectation_z_all_noalloc(const void* d_amplitudes, uint32_t nu
 NqpuCircuit* nqpu_circuit_create_ex(uint32_t num_qubits);
 /* Run with an explicit engine mode. */
 NqpuError    nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode);
+/* Circuit optimizer pre-pass (CircuitOptimizer, circuits/synthesis/
+ * circuit_optimizer.rs:115-735): rewrites the circuit's gate list in place.
+ * Levels as the reference's OptimizationLevel: NONE; BASIC = self-inverse
+ * cancellation, rotation merging, 1q gate fusion; MODERATE = + commutation;
+ * AGGRESSIVE = + peephole patterns.  stats (optional, len values up to 6):
+ * original gates, optimized gates, removed, fusions, commutations, cancellations. */
+typedef enum { NQPU_OPT_NONE = 0, NQPU_OPT_BASIC = 1, NQPU_OPT_MODERATE = 2, NQPU_OPT_AGGRESSIVE = 3 } NqpuOptLevel;
+NqpuError    nqpu_circuit_optimize(NqpuCircuit* circuit, NqpuOptLevel level, uint64_t* stats, uint32_t len);
+/* Read gate `index` back: code (the engine's gate-code order, as the Python
+ * package's GATE_CODES), qubits[3], params[4], matrix[16] (custom gates). */
+NqpuError    nqpu_circuit_get_gate(const NqpuCircuit* circuit, uint32_t index, uint32_t* code, int32_t* qubits,
+                                   double* params, NqpuComplex* matrix);
+
 /* Mid-circuit measurement (QuantumSimulator::measure_qubit, lib.rs:1835) and
  * OpenQASM reset: the circuit runs as segments between them; a measurement
  * collapses the state with the next draw of the thread-local RNG (as

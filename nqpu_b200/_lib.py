@@ -46,6 +46,7 @@ _SCALARS = {
     "NqpuMode": C.c_int,
     "NqpuBatchParam": C.c_int,
     "NqpuRequestKind": C.c_int,
+    "NqpuOptLevel": C.c_int,
     "NqpuServerConfig": NqpuServerConfig,
     "int32_t": C.c_int32,
     "NqpuComplex": NqpuComplex,

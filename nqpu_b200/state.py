@@ -276,6 +276,35 @@ class Circuit:
     def execute(self, state: StateVector, mode: str = "tiled"):
         check(self.lib.nqpu_circuit_execute_ex(self.h_, state.h_, MODES[mode]), "circuit_execute")
 
+    def optimize(self, level: str = "moderate") -> dict:
+        """Rewrite the gate list with the optimizer pre-pass (nqpu_circuit_optimize)."""
+        lv = {"none": 0, "basic": 1, "moderate": 2, "aggressive": 3}[level]
+        st = (C.c_uint64 * 6)()
+        check(self.lib.nqpu_circuit_optimize(self.h_, lv, st, 6), "circuit_optimize")
+        keys = ("original_gates", "optimized_gates", "gates_removed", "fusions", "commutations", "cancellations")
+        return {k: int(v) for k, v in zip(keys, st)}
+
+    def gates(self) -> list:
+        """The gate list as (name, qubits, params[, matrix]) tuples (nqpu_circuit_get_gate)."""
+        from .circuits import GATE_CODES, MID_GATES
+        names = {v: k for k, v in GATE_CODES.items()}
+        out = []
+        code = C.c_uint32()
+        qs = (C.c_int32 * 3)()
+        ps = (C.c_double * 4)()
+        mx = (NqpuComplex * 16)()
+        for i in range(self.gate_count):
+            check(self.lib.nqpu_circuit_get_gate(self.h_, i, C.byref(code), qs, ps, mx), "circuit_get_gate")
+            name = names[code.value]
+            ar = 1 if name in MID_GATES else ARITY[name]
+            g = (name, tuple(int(q) for q in qs[:ar]), tuple(float(p) for p in ps[:NPARAMS[name]]))
+            if name in ("custom1", "custom2", "u2lo"):
+                k = 4 if name == "custom1" else 16
+                m = np.array([complex(mx[j].re, mx[j].im) for j in range(k)])
+                g = g + (m.reshape(2, 2) if k == 4 else m.reshape(4, 4),)
+            out.append(g)
+        return out
+
     def execute_measured(self, state: StateVector, mode: str = "tiled") -> np.ndarray:
         """Execute and return the outcomes of the mid-circuit measurements in order."""
         nmeas = 64 + self.gate_count
