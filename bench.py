@@ -254,6 +254,16 @@ def run_engine(args):
                 "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
                 "launches_per_step": stats["passes"], "avg_launch_ms": avg_launch_ms,
                 "pass_time_share": (sum(launch_ms) / el_ms) if el_ms else None}
+    # the tiled pass is bound by FP32 issue, not HBM: its arithmetic rate against
+    # the FP32 peak (148 SMs x 128 lanes x 2 flops per cycle at the sampled clock)
+    from nqpu_b200.circuits import algorithmic_flops
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    pass_s = sum(launch_ms) / 1000.0 if launch_ms else float("nan")
+    fl = algorithmic_flops(gates, n) * args.steps
+    roofline["fp32"] = {"achieved_tflops": fl / pass_s / 1e12, "peak_tflops": fp32_peak,
+                        "frac": fl / pass_s / 1e12 / fp32_peak, "flops_per_step": fl // args.steps,
+                        "peak_kind": "nominal at the sampled SM clock"}
     launches_per_step = stats["passes"] + 1 + 2  # passes + reset + zsums (2 kernels)
 
     extra = {}

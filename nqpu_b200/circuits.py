@@ -85,6 +85,20 @@ def algorithmic_bytes(gates, n: int, amp_bytes: int) -> int:
     return tot
 
 
+def algorithmic_flops(gates, n: int) -> int:
+    """FP32 flops (an FMA counts two) of the plainest formulation of each gate:
+    a dense 2x2 complex matrix on an amplitude pair takes 8 FMAs per output
+    amplitude (16 flops), a full diagonal one complex product per amplitude (8),
+    a phase on the |1> half 4 per amplitude, a controlled dense 1q gate 8, a
+    dense 4x4 32; permutations and sign flips (X, CNOT, SWAP, Z, CZ, Toffoli,
+    CCZ, CSWAP) none."""
+    per_amp = {"z": 0, "x": 0, "cx": 0, "swap": 0, "cz": 0, "ccx": 0, "ccz": 0, "cswap": 0,
+               "s": 4, "t": 4, "p": 4, "cp": 2, "rz": 8, "rzz": 8,
+               "crx": 8, "cry": 8, "crz": 4, "cu": 8,
+               "iswap": 32, "rxx": 32, "ryy": 32, "custom2": 32}
+    return sum(per_amp.get(g[0], 16) for g in gates) << n
+
+
 # ---------------------------------------------------------------------------
 # Workload generators
 # ---------------------------------------------------------------------------
