@@ -25,7 +25,9 @@
 // contiguous bytes per 16-byte instruction; the (row, column) of every
 // amplitude in A (and D) follows from the same bits.  The output rows are
 // staged through shared memory to make the stores coalesced as well.  Two CTAs
-// share an SM, so one CTA's HBM traffic overlaps the other's MMAs.
+// of eight warps share an SM, so one CTA's HBM traffic overlaps the other's
+// MMAs, and four warps per scheduler hide the latencies of the operand split
+// and the epilogue.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -44,7 +46,10 @@ namespace nqpu {
 // ---------------------------------------------------------------------------
 // Device kernel
 // ---------------------------------------------------------------------------
-constexpr int kFusedThreads = 128;         // one thread per group row (M = 128)
+constexpr int kFusedThreads = 256;         // two threads per group row (M = 128): column halves
+constexpr int kTidBits = 8;                // log2(kFusedThreads)
+constexpr int kLoadSteps = 4096 / (2 * kFusedThreads);  // 16-byte loads per thread per tile
+static_assert((1 << kTidBits) == kFusedThreads && kLoadSteps == 8, "fused tile decomposition");
 constexpr int kAtomBytes = 128 * 128;      // one K-atom (32 tf32) of 128 rows
 constexpr int kAPlane = 2 * kAtomBytes;    // 32 KB: 128 rows x 64 tf32
 constexpr int kBPlane = 2 * 64 * 128;      // 16 KB: 64 rows x 64 tf32
@@ -59,7 +64,9 @@ struct FusedArgs {
   int n_out;              // tile-id bits
   int qout[kMaxQubits];   // qubits of tile-id bits
   int lane_over_j;        // 1: F contains qubit 0
-  int sub[12];            // sub-cube qubits ascending (sub[0..6] = 0..6)
+  int rot;                // 1: load step of lane L is (i + L / 8) % 8 (column bit 0 is a step bit)
+  int fperm[5];           // staging swizzle: row bit b (< 5) -> bit fperm[b] of the column XOR
+  int sub[12];            // sub-cube qubits (sub[0..5] = 0..5)
   int sub_row[12];        // >= 0: row (group) bit of sub-cube bit b, else -1
   int sub_col[12];        // >= 0: column (F) bit of sub-cube bit b, else -1
 };
@@ -141,8 +148,9 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   unsigned char* a_lo = base + kAPlane;
   unsigned char* b_hi = base + 2 * kAPlane;
   unsigned char* b_lo = b_hi + kBPlane;
-  uint64_t* it_addr = reinterpret_cast<uint64_t*>(b_lo + kBPlane);  // 16 entries
-  uint32_t* it_rc = reinterpret_cast<uint32_t*>(it_addr + 16);        // 16 entries: row | col << 16
+  uint64_t* it_addr = reinterpret_cast<uint64_t*>(b_lo + kBPlane);  // kLoadSteps entries
+  uint32_t* it_op = reinterpret_cast<uint32_t*>(it_addr + 16);        // kLoadSteps entries: operand offset part
+  uint32_t* it_st = it_op + 16;                                        // kLoadSteps entries: staging index part
   float2* stage = reinterpret_cast<float2*>(a_hi);                    // output staging (reuses A_hi)
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_holder;
@@ -151,8 +159,8 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t mbar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar));
 
-  // Sub-cube index u = h | tid << 1 | i << 8 (h: amplitude in a 16-byte pair,
-  // i: load step).  Global offset, row and column of u are XORs of the parts.
+  // Sub-cube index u = h | tid << 1 | i << (1 + kTidBits) (h: amplitude in a
+  // 16-byte pair, i: load step).  Global offset, row and column of u are XORs of the parts.
   auto part = [&](uint32_t u, uint64_t* addr, uint32_t* row, uint32_t* col) {
     uint64_t a = 0;
     uint32_t r = 0, c = 0;
@@ -166,13 +174,29 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     *row = r;
     *col = c;
   };
-  if (tid < 16) {
+  // staging swizzle: a bit permutation of the low 5 row bits (linear over XOR)
+  auto fmap = [&](uint32_t r) {
+    uint32_t f = 0;
+#pragma unroll
+    for (int b = 0; b < 5; ++b) f |= ((r >> b) & 1u) << A.fperm[b];
+    return f;
+  };
+  // The swizzled operand offset sw128_off(r, 2c) and the staging index
+  // r * 32 + (c ^ fmap(r)) are both GF(2)-linear in the bits of (r, c) (their
+  // fields occupy disjoint bits), so the offset of sub-cube index
+  // u = h | tid << 1 | step << 9 is the XOR of the offsets of its three parts.
+  auto op_off = [&](uint32_t r, uint32_t c) { return sw128_off<128>(r, 2 * c); };
+  auto st_idx = [&](uint32_t r, uint32_t c) { return r * 32 + (c ^ fmap(r)); };
+  if (tid < kLoadSteps) {
     uint64_t a;
     uint32_t r, c;
-    part(uint32_t(tid) << 8, &a, &r, &c);
+    part(uint32_t(tid) << (1 + kTidBits), &a, &r, &c);
     it_addr[tid] = a;
-    it_rc[tid] = r | (c << 16);
+    it_op[tid] = op_off(r, c);
+    it_st[tid] = st_idx(r, c);
   }
+  // load-step rotation by lane group (8 lanes = 128 contiguous bytes stay together)
+  const uint32_t g = A.rot ? uint32_t((lane >> 3) & 3) : 0u;
   uint64_t t_addr;
   uint32_t t_row, t_col, h_row, h_col;
   {
@@ -180,6 +204,10 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     part(uint32_t(tid) << 1, &t_addr, &t_row, &t_col);
     part(1u, &a, &h_row, &h_col);
   }
+  const uint32_t op_t = op_off(t_row, t_col), op_h = op_off(h_row, h_col);
+  const uint32_t st_t = st_idx(t_row, t_col), st_h = st_idx(h_row, h_col);
+  // qubit of tile-id bit `lane` (tile bases are built by a warp-wide OR)
+  const uint64_t lane_bit = lane < A.n_out ? (1ull << A.qout[lane]) : 0ull;
   // B operand (constant for the launch): row n (output real index), col k
   for (int i = tid; i < 64 * 64; i += blockDim.x) {
     const uint32_t r = i >> 6, k = i & 63;
@@ -215,39 +243,48 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
 
   uint32_t phase = 0;
   auto tile_base_of = [&](uint64_t tile) {
-    uint64_t tb = 0;
-    for (int j = 0; j < A.n_out; ++j)
-      if ((tile >> j) & 1ull) tb |= 1ull << A.qout[j];
-    return tb;
+    const uint64_t mine = ((tile >> lane) & 1ull) ? lane_bit : 0ull;
+    const uint32_t lo = __reduce_or_sync(0xffffffffu, uint32_t(mine));
+    const uint32_t hi = __reduce_or_sync(0xffffffffu, uint32_t(mine >> 32));
+    return uint64_t(lo) | (uint64_t(hi) << 32);
   };
   // tile base tb has no sub-cube bits, and sub-cube bit 0 is qubit 0, so the
   // pair (u, u + 1) is one 16-byte-aligned float4
-  auto load_tile = [&](uint64_t tb, float4 (&v)[16]) {
+  auto load_tile = [&](uint64_t tb, float4 (&v)[kLoadSteps]) {
     const float4* src4 = reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(amp) + tb + t_addr);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __ldcs(src4 + (it_addr[i] >> 1));
+    for (int i = 0; i < kLoadSteps; ++i) v[i] = __ldcs(src4 + (it_addr[(uint32_t(i) + g) & 7u] >> 1));
   };
   // HBM -> A_hi / A_lo (split), swizzled K-major rows; (re, im) = columns
   // (2j, 2j + 1) share one aligned 8-byte slot of a 16-byte chunk
-  auto put = [&](uint32_t row, uint32_t j, float re, float im) {
-    const uint32_t o0 = sw128_off<128>(row, 2 * j);
+  auto put = [&](uint32_t o0, float re, float im) {
     const float hr = tf32_rn(re), hi_ = tf32_rn(im);
     *reinterpret_cast<float2*>(a_hi + o0) = make_float2(hr, hi_);
     *reinterpret_cast<float2*>(a_lo + o0) = make_float2(tf32_rn(re - hr), tf32_rn(im - hi_));
   };
+  // qubit 0 a column bit: the pair (u, u + 1) is columns (j, j + 1) of one
+  // row, j even, i.e. one 16-byte chunk of the swizzled layout
+  auto put2 = [&](uint32_t o0, float4 x) {
+    const float4 h = make_float4(tf32_rn(x.x), tf32_rn(x.y), tf32_rn(x.z), tf32_rn(x.w));
+    *reinterpret_cast<float4*>(a_hi + o0) = h;
+    *reinterpret_cast<float4*>(a_lo + o0) =
+        make_float4(tf32_rn(x.x - h.x), tf32_rn(x.y - h.y), tf32_rn(x.z - h.z), tf32_rn(x.w - h.w));
+  };
   // software pipeline: the next tile's HBM loads are in flight while the
   // current tile's MMAs, epilogue and stores run
-  float4 v[16];
+  float4 v[kLoadSteps];
   if (uint64_t(blockIdx.x) < n_tiles) load_tile(tile_base_of(blockIdx.x), v);
   for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const uint64_t tb = tile_base_of(tile);
-    {
+    if (A.lane_over_j) {
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const uint32_t rc = it_rc[i];
-        const uint32_t r0 = t_row | (rc & 0xFFFFu), c0 = t_col | (rc >> 16);
-        put(r0, c0, v[i].x, v[i].y);
-        put(r0 | h_row, c0 | h_col, v[i].z, v[i].w);
+      for (int i = 0; i < kLoadSteps; ++i) put2(op_t ^ it_op[(uint32_t(i) + g) & 7u], v[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < kLoadSteps; ++i) {
+        const uint32_t o0 = op_t ^ it_op[(uint32_t(i) + g) & 7u];
+        put(o0, v[i].x, v[i].y);
+        put(o0 ^ op_h, v[i].z, v[i].w);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -286,33 +323,31 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
-    // TMEM -> registers: warp w reads lanes 32w..32w+31, thread = row
-    uint32_t r[64];
-    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+    // TMEM -> registers: warp w reads lanes 32 (w % 4) .. + 31 (row = tid % 128)
+    // and the fp32 columns 32 (w / 4) .. + 31 (complex columns 16 (w / 4) .. + 15)
+    uint32_t r[32];
+    const uint32_t row = uint32_t(tid) & 127u, jb = uint32_t(warp >> 2) * 16u;
+    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + 2u * jb;
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
-        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
-        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
-          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
-          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
-          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
-          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 
-    // row tid of D -> staging (row-major, column index XOR-swizzled by row)
+    // (row, j) of D -> staging (row-major, column index XOR-swizzled by fmap(row))
+    const uint32_t frow = fmap(row);
     double tile_norm = 0.0;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const float2 o = make_float2(__uint_as_float(r[2 * j]) * scale, __uint_as_float(r[2 * j + 1]) * scale);
+    for (int jj = 0; jj < 16; ++jj) {
+      const uint32_t j = jb + uint32_t(jj);
+      const float2 o = make_float2(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale);
       tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
-      stage[tid * 32 + (j ^ (tid & 31))] = o;
+      stage[row * 32 + (j ^ frow)] = o;
     }
     norm_acc += tile_norm;
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -321,13 +356,12 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     {
       float4* dst4 = reinterpret_cast<float4*>(reinterpret_cast<float2*>(amp) + tb + t_addr);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const uint32_t rc = it_rc[i];
-        const uint32_t r0 = t_row | (rc & 0xFFFFu), c0 = t_col | (rc >> 16);
-        const uint32_t r1 = r0 | h_row, c1 = c0 | h_col;
-        const float2 o0 = stage[r0 * 32 + (c0 ^ (r0 & 31))];
-        const float2 o1 = stage[r1 * 32 + (c1 ^ (r1 & 31))];
-        __stcs(dst4 + (it_addr[i] >> 1), make_float4(o0.x, o0.y, o1.x, o1.y));
+      for (int i = 0; i < kLoadSteps; ++i) {
+        const uint32_t st = (uint32_t(i) + g) & 7u;
+        const uint32_t i0 = st_t ^ it_st[st];
+        const float2 o0 = stage[i0];
+        const float2 o1 = stage[i0 ^ st_h];
+        __stcs(dst4 + (it_addr[st] >> 1), make_float4(o0.x, o0.y, o1.x, o1.y));
       }
     }
     __syncthreads();  // the A planes (and the staging area in A_hi) are refilled next tile
@@ -394,26 +428,88 @@ static FusedArgs make_args(const FusedGate& g, int n) {
   for (int q = 0; q < n && ng < 7; ++q)
     if (!((F >> q) & 1)) { a.gq[ng++] = q; G |= 1ull << q; }
   a.ng = ng;
+  // Row order of the group qubits.  The operand store of amplitude (row r,
+  // column c) lands in the 8-byte bank slot (c & 1) | (((c >> 1) ^ r) & 7) << 1
+  // of the 128-byte-swizzled layout, and the lanes of a warp run over qubits
+  // 1..5.  Row bits 0..2 are given to lane qubits wherever the matching column
+  // bit (c bits 1..3) is not a lane qubit, so that the lanes of one store phase
+  // (a quarter warp for the 16-byte stores used when qubit 0 is a column bit,
+  // a half warp for the 8-byte ones otherwise) hit distinct slots.
+  {
+    const int wmax = (F & 1ull) ? 3 : 4;  // lane qubits 1..wmax share one store phase
+    auto in_w = [&](int q) { return q >= 1 && q <= wmax; };
+    int order[7];
+    bool used[7] = {false, false, false, false, false, false, false};
+    int no = 0;
+    for (int k = 0; k < 3 && k < ng; ++k) {
+      const bool col_is_lane = k + 1 < 5 && in_w(a.q[k + 1]);
+      int pick = -1;
+      for (int i = 0; i < ng && pick < 0; ++i)
+        if (!used[i] && in_w(a.gq[i]) != col_is_lane) pick = i;
+      for (int i = 0; i < ng && pick < 0; ++i)
+        if (!used[i]) pick = i;
+      used[pick] = true;
+      order[no++] = a.gq[pick];
+    }
+    for (int i = 0; i < ng; ++i)
+      if (!used[i]) order[no++] = a.gq[i];
+    for (int i = 0; i < ng; ++i) a.gq[i] = order[i];
+  }
   int no = 0;
   for (int q = 0; q < n; ++q)
     if (!(((F | G) >> q) & 1)) a.qout[no++] = q;
   a.n_out = no;
   a.lane_over_j = (F & 1ull) ? 1 : 0;
-  // sub-cube bits in ascending qubit order
+  // Sub-cube bits: 0..5 are qubits 0..5 (16-byte pairs, lanes: 512 contiguous
+  // bytes per warp), 6..8 the warp bits, 9..11 the load steps.  When column
+  // bit 0 (the lowest fused qubit) is not a lane qubit it becomes step bit 0
+  // and lane groups run the steps rotated, so that one store covers both
+  // column parities.
   int nb = 0;
-  for (int q = 0; q < n && nb < 12; ++q) {
-    if (!(((F | G) >> q) & 1)) continue;
-    a.sub[nb] = q;
-    a.sub_row[nb] = -1;
-    a.sub_col[nb] = -1;
+  for (int q = 0; q < n && nb < 12; ++q)
+    if (((F | G) >> q) & 1) a.sub[nb++] = q;
+  a.rot = 0;
+  if (a.q[0] >= 6) {
+    int at = -1;
+    for (int b = 6; b < 12; ++b)
+      if (a.sub[b] == a.q[0]) at = b;
+    std::swap(a.sub[at], a.sub[9]);
+    a.rot = 1;
+  }
+  for (int b = 0; b < 12; ++b) {
+    const int q = a.sub[b];
+    a.sub_row[b] = -1;
+    a.sub_col[b] = -1;
     if ((F >> q) & 1) {
       for (int i = 0; i < 5; ++i)
-        if (a.q[i] == q) a.sub_col[nb] = i;
+        if (a.q[i] == q) a.sub_col[b] = i;
     } else {
       for (int i = 0; i < ng; ++i)
-        if (a.gq[i] == q) a.sub_row[nb] = i;
+        if (a.gq[i] == q) a.sub_row[b] = i;
     }
-    ++nb;
+  }
+  // Staging swizzle: the output tile is staged row-major with column c of row
+  // r at c ^ fmap(r); its 8-byte bank slot is (c ^ fmap(r)) & 15.  Each of the
+  // slot bits 0..3 pairs with a row bit that varies across the lanes of the
+  // store phase's loads exactly when the column bit does not.
+  {
+    auto varies = [&](int q) {
+      if (q >= 1 && q <= 5) return true;
+      return a.rot && (q == a.sub[9] || q == a.sub[10]);
+    };
+    bool used[5] = {false, false, false, false, false};
+    for (int t = 0; t < 4; ++t) {
+      const bool cv = varies(a.q[t]);
+      int pick = -1;
+      for (int b = 0; b < 5 && pick < 0; ++b)
+        if (!used[b] && varies(a.gq[b]) != cv) pick = b;
+      for (int b = 0; b < 5 && pick < 0; ++b)
+        if (!used[b]) pick = b;
+      used[pick] = true;
+      a.fperm[pick] = t;
+    }
+    for (int b = 0; b < 5; ++b)
+      if (!used[b]) a.fperm[b] = 4;
   }
   return a;
 }
