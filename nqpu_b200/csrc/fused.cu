@@ -20,11 +20,13 @@
 // Operands live in shared memory in the K-major 128-byte-swizzled layout.
 //
 // HBM access: a tile's 4096 amplitudes form a 12-dimensional sub-cube (F and
-// the 7 lowest qubits outside F, which always include qubits 0..6).  Loads and
-// stores walk the sub-cube in its own linear order, so each warp moves 512
-// contiguous bytes per 16-byte instruction; the (row, column) of every
-// amplitude in A (and D) follows from the same bits.  The output rows are
-// staged through shared memory to make the stores coalesced as well.  Two CTAs
+// the 7 lowest qubits outside F, which always include qubits 0..6).  Loads
+// walk the sub-cube in its own linear order, so each warp moves 512 contiguous
+// bytes per 16-byte instruction; the (row, column) of every amplitude in A
+// follows from the same bits.  Results go from tensor memory straight to HBM:
+// a warp's lanes hold 32 rows of D, whose low row bits the group-row order
+// gives to the unfused qubits among 0..4, so that the stores stay coalesced
+// (32 neighbouring amplitudes when none of qubits 0..4 is fused).  Two CTAs
 // of eight warps share an SM, so one CTA's HBM traffic overlaps the other's
 // MMAs, and four warps per scheduler hide the latencies of the operand split
 // and the epilogue.
@@ -65,7 +67,6 @@ struct FusedArgs {
   int qout[kMaxQubits];   // qubits of tile-id bits
   int lane_over_j;        // 1: F contains qubit 0
   int rot;                // 1: load step of lane L is (i + L / 8) % 8 (column bit 0 is a step bit)
-  int fperm[5];           // staging swizzle: row bit b (< 5) -> bit fperm[b] of the column XOR
   int sub[12];            // sub-cube qubits (sub[0..5] = 0..5)
   int sub_row[12];        // >= 0: row (group) bit of sub-cube bit b, else -1
   int sub_col[12];        // >= 0: column (F) bit of sub-cube bit b, else -1
@@ -150,8 +151,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   unsigned char* b_lo = b_hi + kBPlane;
   uint64_t* it_addr = reinterpret_cast<uint64_t*>(b_lo + kBPlane);  // kLoadSteps entries
   uint32_t* it_op = reinterpret_cast<uint32_t*>(it_addr + 16);        // kLoadSteps entries: operand offset part
-  uint32_t* it_st = it_op + 16;                                        // kLoadSteps entries: staging index part
-  float2* stage = reinterpret_cast<float2*>(a_hi);                    // output staging (reuses A_hi)
+  uint64_t* ctab = reinterpret_cast<uint64_t*>(it_op + 16);           // 32 entries: amplitude offset of column j
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_holder;
   __shared__ int abort_flag;
@@ -174,26 +174,22 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     *row = r;
     *col = c;
   };
-  // staging swizzle: a bit permutation of the low 5 row bits (linear over XOR)
-  auto fmap = [&](uint32_t r) {
-    uint32_t f = 0;
-#pragma unroll
-    for (int b = 0; b < 5; ++b) f |= ((r >> b) & 1u) << A.fperm[b];
-    return f;
-  };
-  // The swizzled operand offset sw128_off(r, 2c) and the staging index
-  // r * 32 + (c ^ fmap(r)) are both GF(2)-linear in the bits of (r, c) (their
-  // fields occupy disjoint bits), so the offset of sub-cube index
-  // u = h | tid << 1 | step << 9 is the XOR of the offsets of its three parts.
+  // The swizzled operand offset sw128_off(r, 2c) is GF(2)-linear in the bits
+  // of (r, c) (its fields occupy disjoint bits), so the offset of sub-cube
+  // index u = h | tid << 1 | step << 9 is the XOR of the offsets of its parts.
   auto op_off = [&](uint32_t r, uint32_t c) { return sw128_off<128>(r, 2 * c); };
-  auto st_idx = [&](uint32_t r, uint32_t c) { return r * 32 + (c ^ fmap(r)); };
   if (tid < kLoadSteps) {
     uint64_t a;
     uint32_t r, c;
     part(uint32_t(tid) << (1 + kTidBits), &a, &r, &c);
     it_addr[tid] = a;
     it_op[tid] = op_off(r, c);
-    it_st[tid] = st_idx(r, c);
+  }
+  if (tid < 32) {
+    uint64_t o = 0;
+    for (int b = 0; b < 5; ++b)
+      if ((tid >> b) & 1) o |= 1ull << A.q[b];
+    ctab[tid] = o;
   }
   // load-step rotation by lane group (8 lanes = 128 contiguous bytes stay together)
   const uint32_t g = A.rot ? uint32_t((lane >> 3) & 3) : 0u;
@@ -205,7 +201,10 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     part(1u, &a, &h_row, &h_col);
   }
   const uint32_t op_t = op_off(t_row, t_col), op_h = op_off(h_row, h_col);
-  const uint32_t st_t = st_idx(t_row, t_col), st_h = st_idx(h_row, h_col);
+  // amplitude offset of this thread's output row (row = tid % 128: its TMEM lane)
+  uint64_t row_addr = 0;
+  for (int b = 0; b < 12; ++b)
+    if (A.sub_row[b] >= 0 && ((uint32_t(tid & 127) >> A.sub_row[b]) & 1u)) row_addr |= 1ull << A.sub[b];
   // qubit of tile-id bit `lane` (tile bases are built by a warp-wide OR)
   const uint64_t lane_bit = lane < A.n_out ? (1ull << A.qout[lane]) : 0ull;
   // B operand (constant for the launch): row n (output real index), col k
@@ -339,33 +338,32 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 
-    // (row, j) of D -> staging (row-major, column index XOR-swizzled by fmap(row))
-    const uint32_t frow = fmap(row);
+    // row of D -> HBM directly: the warp's 32 rows are the thread rows; when
+    // qubit 0 is fused, columns (j, j + 1) are adjacent amplitudes (16 bytes)
     double tile_norm = 0.0;
+    float2* out = reinterpret_cast<float2*>(amp) + tb + row_addr;
+    if (A.lane_over_j) {
 #pragma unroll
-    for (int jj = 0; jj < 16; ++jj) {
-      const uint32_t j = jb + uint32_t(jj);
-      const float2 o = make_float2(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale);
-      tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
-      stage[row * 32 + (j ^ frow)] = o;
-    }
-    norm_acc += tile_norm;
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();  // staging complete; TMEM free for the next tile
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    {
-      float4* dst4 = reinterpret_cast<float4*>(reinterpret_cast<float2*>(amp) + tb + t_addr);
+      for (int jj = 0; jj < 16; jj += 2) {
+        const float4 o = make_float4(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale,
+                                     __uint_as_float(r[2 * jj + 2]) * scale, __uint_as_float(r[2 * jj + 3]) * scale);
+        tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y) + double(o.z) * double(o.z) +
+                     double(o.w) * double(o.w);
+        __stcs(reinterpret_cast<float4*>(out + ctab[jb + uint32_t(jj)]), o);
+      }
+    } else {
 #pragma unroll
-      for (int i = 0; i < kLoadSteps; ++i) {
-        const uint32_t st = (uint32_t(i) + g) & 7u;
-        const uint32_t i0 = st_t ^ it_st[st];
-        const float2 o0 = stage[i0];
-        const float2 o1 = stage[i0 ^ st_h];
-        __stcs(dst4 + (it_addr[st] >> 1), make_float4(o0.x, o0.y, o1.x, o1.y));
+      for (int jj = 0; jj < 16; ++jj) {
+        const float2 o = make_float2(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale);
+        tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+        __stcs(out + ctab[jb + uint32_t(jj)], o);
       }
     }
-    __syncthreads();  // the A planes (and the staging area in A_hi) are refilled next tile
+    norm_acc += tile_norm;
+    // TMEM is read and the MMAs are complete: the next tile's operand split
+    // may start; the barrier after it orders these reads before the next MMAs
   }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   // per-CTA FP64 norm partial (fixed-order tree: warp shuffles, then warp 0)
   __shared__ double wsum[kFusedThreads / 32];
   double nsum = norm_acc;
@@ -373,6 +371,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   for (int o = 16; o > 0; o >>= 1) nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
   if (lane == 0) wsum[warp] = nsum;
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (tid == 0) {
     double t = 0.0;
     for (int w = 0; w < kFusedThreads / 32; ++w) t += wsum[w];
@@ -487,29 +486,6 @@ static FusedArgs make_args(const FusedGate& g, int n) {
       for (int i = 0; i < ng; ++i)
         if (a.gq[i] == q) a.sub_row[b] = i;
     }
-  }
-  // Staging swizzle: the output tile is staged row-major with column c of row
-  // r at c ^ fmap(r); its 8-byte bank slot is (c ^ fmap(r)) & 15.  Each of the
-  // slot bits 0..3 pairs with a row bit that varies across the lanes of the
-  // store phase's loads exactly when the column bit does not.
-  {
-    auto varies = [&](int q) {
-      if (q >= 1 && q <= 5) return true;
-      return a.rot && (q == a.sub[9] || q == a.sub[10]);
-    };
-    bool used[5] = {false, false, false, false, false};
-    for (int t = 0; t < 4; ++t) {
-      const bool cv = varies(a.q[t]);
-      int pick = -1;
-      for (int b = 0; b < 5 && pick < 0; ++b)
-        if (!used[b] && varies(a.gq[b]) != cv) pick = b;
-      for (int b = 0; b < 5 && pick < 0; ++b)
-        if (!used[b]) pick = b;
-      used[pick] = true;
-      a.fperm[pick] = t;
-    }
-    for (int b = 0; b < 5; ++b)
-      if (!used[b]) a.fperm[b] = 4;
   }
   return a;
 }

@@ -41,6 +41,29 @@ def test_fused_random_circuits(n):
     assert np.abs(sv.expectation_z_all() - o.expectation_z_all()).max() <= TOL
 
 
+# Fused qubit sets that take each operand-layout case of the kernel: qubit 0
+# fused (16-byte operand stores), lane qubits 1..5 fused without qubit 0,
+# lowest fused qubit at 6 or above (rotated load steps), and mixtures.
+@pytest.mark.parametrize("fset", [(0, 1, 2, 3, 4), (0, 2, 9, 10, 11), (1, 2, 10, 11, 12), (3, 6, 7, 12, 13),
+                                  (5, 6, 7, 8, 9), (6, 7, 8, 9, 10), (9, 10, 11, 12, 13)])
+def test_fused_operand_layouts(fset):
+    n = 14
+    rng = np.random.default_rng(sum(fset))
+    gates = [("u3", (q,), tuple(rng.uniform(0, 6, 3))) for q in range(n)]
+    # dense gates confined to the five qubits: one fused unitary on exactly fset
+    for _ in range(12):
+        a, b = (int(x) for x in rng.choice(fset, size=2, replace=False))
+        gates.append(("cx", (a, b), ()))
+        gates.append(("u3", (b,), tuple(rng.uniform(0, 6, 3))))
+        gates.append(("rzz", (a, b), (float(rng.uniform(-3, 3)),)))
+    sv = StateVector(n, "c64")
+    Circuit(n, gates).execute(sv, "fused")
+    o = OracleState(n)
+    o.apply(gates)
+    assert 1 - fid(sv.amplitudes(), o.amplitudes()) <= TOL
+    assert np.abs(sv.expectation_z_all() - o.expectation_z_all()).max() <= TOL
+
+
 @pytest.mark.parametrize("n", [12, 17])
 def test_fused_brickwork_and_modes_agree(n):
     gates = circuits.brickwork(n, 12, seed=n)
