@@ -254,6 +254,14 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
 #pragma unroll
     for (int i = 0; i < kLoadSteps; ++i) v[i] = __ldcs(src4 + (it_addr[(uint32_t(i) + g) & 7u] >> 1));
   };
+  // the tile after the next one is pulled into L2 meanwhile (no registers or
+  // shared memory held), so the next loads meet L2 rather than DRAM latency
+  auto prefetch_tile = [&](uint64_t tb) {
+    const float4* src4 = reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(amp) + tb + t_addr);
+#pragma unroll
+    for (int i = 0; i < kLoadSteps; ++i)
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(src4 + (it_addr[(uint32_t(i) + g) & 7u] >> 1)));
+  };
   // HBM -> A_hi / A_lo (split), swizzled K-major rows; (re, im) = columns
   // (2j, 2j + 1) share one aligned 8-byte slot of a 16-byte chunk
   auto put = [&](uint32_t o0, float re, float im) {
@@ -273,6 +281,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   // current tile's MMAs, epilogue and stores run
   float4 v[kLoadSteps];
   if (uint64_t(blockIdx.x) < n_tiles) load_tile(tile_base_of(blockIdx.x), v);
+  if (uint64_t(blockIdx.x) + gridDim.x < n_tiles) prefetch_tile(tile_base_of(blockIdx.x + gridDim.x));
   for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const uint64_t tb = tile_base_of(tile);
     if (A.lane_over_j) {
@@ -306,6 +315,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
                    : "memory");
     }
     if (tile + gridDim.x < n_tiles) load_tile(tile_base_of(tile + gridDim.x), v);
+    if (tile + 2ull * gridDim.x < n_tiles) prefetch_tile(tile_base_of(tile + 2ull * gridDim.x));
     // bounded wait for the MMAs
     {
       uint32_t it = 0;
