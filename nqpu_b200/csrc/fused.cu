@@ -254,8 +254,8 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
 #pragma unroll
     for (int i = 0; i < kLoadSteps; ++i) v[i] = __ldcs(src4 + (it_addr[(uint32_t(i) + g) & 7u] >> 1));
   };
-  // the tile after the next one is pulled into L2 meanwhile (no registers or
-  // shared memory held), so the next loads meet L2 rather than DRAM latency
+  // the tiles two and three ahead are pulled into L2 meanwhile (no registers
+  // or shared memory held), so the next loads meet L2 rather than DRAM latency
   auto prefetch_tile = [&](uint64_t tb) {
     const float4* src4 = reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(amp) + tb + t_addr);
 #pragma unroll
@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   float4 v[kLoadSteps];
   if (uint64_t(blockIdx.x) < n_tiles) load_tile(tile_base_of(blockIdx.x), v);
   if (uint64_t(blockIdx.x) + gridDim.x < n_tiles) prefetch_tile(tile_base_of(blockIdx.x + gridDim.x));
+  if (uint64_t(blockIdx.x) + 2ull * gridDim.x < n_tiles) prefetch_tile(tile_base_of(blockIdx.x + 2ull * gridDim.x));
   for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const uint64_t tb = tile_base_of(tile);
     if (A.lane_over_j) {
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
                    : "memory");
     }
     if (tile + gridDim.x < n_tiles) load_tile(tile_base_of(tile + gridDim.x), v);
-    if (tile + 2ull * gridDim.x < n_tiles) prefetch_tile(tile_base_of(tile + 2ull * gridDim.x));
+    if (tile + 3ull * gridDim.x < n_tiles) prefetch_tile(tile_base_of(tile + 3ull * gridDim.x));
     // bounded wait for the MMAs
     {
       uint32_t it = 0;
