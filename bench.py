@@ -139,7 +139,8 @@ def run_reference(args):
     value = cnt / el
     cores = O.max_threads()
     line = {
-        "impl": "reference", "metric": "gates/s (30q complex64 brickwork, unfused)", "value": value,
+        "impl": "reference", "metric": f"gates/s ({n}q {'complex64' if f32 else 'complex128'} brickwork, unfused)",
+        "value": value,
         "unit": "gates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64" if f32 else "c128", "data": "synthetic",
@@ -328,7 +329,8 @@ def run_engine(args):
 
     if rank == 0:
         line = {
-            "metric": ("gates/s (30q complex64 brickwork, unfused)" if args.circuit == "brickwork"
+            "metric": (f"gates/s ({n}q {'complex64' if args.dtype == 'c64' else 'complex128'} brickwork, unfused)"
+                       if args.circuit == "brickwork"
                        else f"gates/s ({n}q QFT, unfused)"), "value": value, "unit": "gates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak",
