@@ -263,6 +263,18 @@ static TileOp<Real> encode_op(const Op& o, const int* tile_pos, const int* reg_o
     t.m[2 * i] = Real(o.m[i].real());
     t.m[2 * i + 1] = Real(o.m[i].imag());
   }
+  // flat dispatch code: 1 + b for a dense 1q gate on register bit b without
+  // register controls, 8 + 8 b + v for X on register bit b with at most one
+  // register control (v = 0: none, else its register bit + 1)
+  if (o.kind == OP_U1 && t.creg == 0) t.fast = uint8_t(1 + t.rb0);
+  if (o.kind == OP_X1 && (t.creg & (t.creg - 1)) == 0) {
+    int v = 0;
+    if (t.creg) {
+      v = 1;
+      while (!((t.creg >> (v - 1)) & 1u)) ++v;
+    }
+    t.fast = uint8_t(8 + 8 * t.rb0 + v);
+  }
   return t;
 }
 

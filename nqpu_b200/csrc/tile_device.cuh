@@ -342,6 +342,26 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
     const uint32_t dv0 = h0.w;
     const bool tc = (vbase & cnr) == cnr;
     const Real* mp = op->m;
+    // the common cases (dense 1q gate, X / CNOT with at most one register
+    // control) through one flat switch on a code the planner precomputed
+    const uint32_t fast = (h0.y >> 16) & 0xFF;
+    if (fast != 0) {
+      switch (fast) {
+#define NQ_FU1(B, _) case 1 + B: if constexpr (B < NRB) { if (tc) rb_u1<C, NA, B>(a, pm0, pm1, pm2, pm3); } break;
+        NQ_REG_CASES(NQ_FU1, 0)
+#undef NQ_FU1
+#define NQ_FX1V(B, V) case 8 + 8 * B + V: \
+        if constexpr (B < NRB && (V == 0 || (V - 1 < NRB && V - 1 != B))) \
+          rb_x1_fixed<C, NA, B, (V == 0 ? 0 : (1 << (V - 1))), false>(a, tc); \
+        break;
+#define NQ_FX1(B, _) NQ_FX1V(B, 0) NQ_FX1V(B, 1) NQ_FX1V(B, 2) NQ_FX1V(B, 3) NQ_FX1V(B, 4) NQ_FX1V(B, 5)
+        NQ_REG_CASES(NQ_FX1, 0)
+#undef NQ_FX1
+#undef NQ_FX1V
+        default: break;
+      }
+      continue;
+    }
     switch (kind) {
       case OP_U1: {
         const C m0 = pm0, m1 = pm1, m2 = pm2, m3 = pm3;
