@@ -439,9 +439,11 @@ def run_batch(args):
     torch.cuda.set_device(dev)
     count = args.circuits
     items = hea_batch(count, args.seed, nmin=10, nmax=22, lmin=2, lmax=12)
+    # the same circuits as flat gate arrays (the input of Circuit.from_arrays)
+    arrs = hea_batch(count, args.seed, nmin=10, nmax=22, lmin=2, lmax=12, arrays=True)
     G = sum(len(g) for _, g, _, _ in items)
     t0 = time.perf_counter()
-    circs = [Circuit(n, g) for n, g, _, _ in items]
+    circs = [Circuit.from_arrays(n, *a) for n, a, _, _ in arrs]
     host_build_s = time.perf_counter() - t0
     log = (lambda m: print(m, file=sys.stderr, flush=True)) if args.verbose else None
     if args.quick:  # timed region only: library defaults, no tuning
@@ -521,11 +523,11 @@ def run_batch(args):
     plain_rate = len(sample) / plain_s if sample else None
     tiled_rate = len(sample) / tiled_s if sample else None
 
-    # e2e through the public API: gate lists -> circuits -> batch -> <H> on the host
+    # e2e through the public API: gate arrays -> circuits -> batch -> <H> on the host
     e2e = None
     if not args.quick:
         t = time.perf_counter()
-        cs = [Circuit(n, g) for n, g, _, _ in items]
+        cs = [Circuit.from_arrays(n, *a) for n, a, _, _ in arrs]
         b2 = Batch()
         b2.config(**cfg)
         for c, (n, g, J, h) in zip(cs, items):
@@ -535,8 +537,8 @@ def run_batch(args):
         assert np.array_equal(r2, res)
         e2e = {"value": count / et, "unit": "circuits/s", "h2d_bytes_per_step": int(st["upload_bytes"]),
                "d2h_bytes_per_step": 8 * count, "seconds_per_step": et,
-               "timing": "host wall clock: Circuit handles from gate lists, batch add, prepare (plans, "
-                         "uploads, graph capture), one replay, results on the host"}
+               "timing": "host wall clock: Circuit handles from gate arrays (Circuit.from_arrays), batch add, "
+                         "prepare (plans on host threads, uploads, graph capture), one replay, results on the host"}
         b2.close()
         for c in cs:
             c.close()

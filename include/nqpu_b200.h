@@ -251,6 +251,16 @@ NqpuError    nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uint32_t q2
 NqpuError   nqpu_expectation_z_all_noalloc(const void* d_amplitudes, uint32_t num_qubits,
                                            NqpuDtype dtype, double* d_out, void* cuda_stream);
 
+/* No counterpart in the reference: the bulk form of the nqpu_circuit_add_*
+ * calls, for callers that build large circuits or many circuits (one call per
+ * circuit instead of one per gate).  Gate i: codes[i] in the gate-code order
+ * of nqpu_circuit_get_gate (measure and reset included), qubits[3i..3i+2] and
+ * params[4i..4i+3] (slots a gate does not use are ignored), matrices[16i..]
+ * row-major for the custom gates only (NULL when there are none; custom 1q
+ * reads the first 4 entries).  Each gate is checked as its single add would
+ * check it; nothing is appended unless all are valid. */
+NqpuError    nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t* codes, const int32_t* qubits,
+                                    const double* params, const NqpuComplex* matrices, uint32_t count);
 /* Like nqpu_circuit_create with the 34-qubit engine limit. */
 NqpuCircuit* nqpu_circuit_create_ex(uint32_t num_qubits);
 /* Run with an explicit engine mode. */

@@ -169,6 +169,29 @@ def hea(n: int, layers: int, rng: np.random.Generator):
     return gates
 
 
+def hea_arrays(n: int, layers: int, rng: np.random.Generator):
+    """hea() as flat arrays (codes [G], qubits [G, 3], params [G, 4]) for
+    Circuit.from_arrays, with the same draws and gate order."""
+    per = 3 * n - 1
+    codes = np.empty(layers * per, dtype=np.uint32)
+    qs = np.zeros((layers * per, 3), dtype=np.int32)
+    ps = np.zeros((layers * per, 4), dtype=np.float64)
+    q = np.arange(n)
+    for layer in range(layers):
+        ang = 2 * math.pi * rng.random((n, 2))
+        b = layer * per
+        codes[b:b + 2 * n:2] = GATE_CODES["ry"]
+        codes[b + 1:b + 2 * n:2] = GATE_CODES["rz"]
+        qs[b:b + 2 * n:2, 0] = q
+        qs[b + 1:b + 2 * n:2, 0] = q
+        ps[b:b + 2 * n:2, 0] = ang[:, 0]
+        ps[b + 1:b + 2 * n:2, 0] = ang[:, 1]
+        codes[b + 2 * n:b + per] = GATE_CODES["cz"]
+        qs[b + 2 * n:b + per, 0] = q[:-1]
+        qs[b + 2 * n:b + per, 1] = q[1:]
+    return codes, qs, ps
+
+
 def ising_hamiltonian(n: int, rng: np.random.Generator):
     """H = sum_i J_i Z_i Z_{i+1} + sum_i h_i X_i with J_i, h_i ~ U[-1, 1]."""
     J = rng.uniform(-1.0, 1.0, n - 1)
@@ -176,15 +199,17 @@ def ising_hamiltonian(n: int, rng: np.random.Generator):
     return J, h
 
 
-def hea_batch(count: int, seed: int, nmin: int = 10, nmax: int = 22, lmin: int = 2, lmax: int = 12):
+def hea_batch(count: int, seed: int, nmin: int = 10, nmax: int = 22, lmin: int = 2, lmax: int = 12,
+              arrays: bool = False):
     """Batch of HEA circuits with their Ising Hamiltonians.  Per circuit, draw
-    order: n ~ U{nmin..nmax}, L ~ U{lmin..lmax}, the ansatz angles, then J, h."""
+    order: n ~ U{nmin..nmax}, L ~ U{lmin..lmax}, the ansatz angles, then J, h.
+    arrays=True gives each circuit as hea_arrays' (codes, qubits, params)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
         n = int(rng.integers(nmin, nmax + 1))
         L = int(rng.integers(lmin, lmax + 1))
-        g = hea(n, L, rng)
+        g = hea_arrays(n, L, rng) if arrays else hea(n, L, rng)
         J, h = ising_hamiltonian(n, rng)
         out.append((n, g, J, h))
     return out

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/nqpu_b200.h"
@@ -91,18 +92,37 @@ static cudaError_t batch_build(BatchImpl* b) {
   uint64_t arena_amps = 0;
   uint32_t counters = 0, partials = 0;
   b->n_small = 0;
-  // per-circuit tiled plans, concatenated with rebased stage/op indices
-  for (size_t ci = 0; ci < b->entries.size(); ++ci) {
+  // per-circuit tiled plans (independent: built on host threads), then
+  // concatenated with rebased stage/op indices
+  const size_t nc = b->entries.size();
+  std::vector<TilePlan> plans(nc);
+  std::vector<char> plan_ok(nc, 0);
+  {
+    auto work = [&](size_t lo, size_t hi) {
+      for (size_t ci = lo; ci < hi; ++ci) {
+        const BatchEntry& E = b->entries[ci];
+        const bool small = E.n <= b->small_max;
+        const int kmax = small ? 13 : std::min(b->plan_kmax, 13);
+        std::string err;
+        plan_ok[ci] = build_tile_plan(lower_circuit(E.gates), E.n, DType::C64, kmax, &plans[ci], &err) &&
+                      (!small || plans[ci].passes.size() == 1);
+      }
+    };
+    const size_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min(hw, std::max<size_t>(1, nc / 64));
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nt; ++t) th.emplace_back(work, nc * t / nt, nc * (t + 1) / nt);
+    work(0, nc / nt);
+    for (auto& x : th) x.join();
+  }
+  for (size_t ci = 0; ci < nc; ++ci) {
     const BatchEntry& E = b->entries[ci];
     BatchCirc& C = circs[ci];
     std::memset(&C, 0, sizeof(C));
     C.n = E.n;
     C.small = E.n <= b->small_max ? 1 : 0;
-    TilePlan tp;
-    std::string err;
-    const int kmax = C.small ? 13 : std::min(b->plan_kmax, 13);
-    if (!build_tile_plan(lower_circuit(E.gates), E.n, DType::C64, kmax, &tp, &err)) return cudaErrorInvalidValue;
-    if (C.small && tp.passes.size() != 1) return cudaErrorInvalidValue;
+    if (!plan_ok[ci]) return cudaErrorInvalidValue;
+    const TilePlan& tp = plans[ci];
     C.pass_base = int32_t(passes.size());
     C.n_passes = int32_t(tp.passes.size());
     const int32_t sbase = int32_t(stages.size()), obase = int32_t(ops.size());

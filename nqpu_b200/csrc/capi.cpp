@@ -498,9 +498,7 @@ extern "C" void nqpu_circuit_destroy(NqpuCircuit* circuit) {
   if (circuit) circuit_free(Cc(circuit));
 }
 
-static NqpuError add_rec(NqpuCircuit* circuit, const GateRec& g) {
-  if (!circuit) return NQPU_NULL_POINTER;
-  CircuitImpl* c = Cc(circuit);
+static NqpuError check_rec(const CircuitImpl* c, const GateRec& g) {
   const int ar = gate_arity(g.code);
   for (int i = 0; i < ar; ++i)
     if (g.q[i] < 0 || uint32_t(g.q[i]) >= c->n) return NQPU_INVALID_QUBIT;
@@ -509,6 +507,14 @@ static NqpuError add_rec(NqpuCircuit* circuit, const GateRec& g) {
       if (g.q[i] == g.q[j]) return NQPU_INVALID_PARAMETER;
   for (int i = 0; i < 4; ++i)
     if (!is_finite_param(g.p[i])) return NQPU_INVALID_PARAMETER;
+  return NQPU_OK;
+}
+
+static NqpuError add_rec(NqpuCircuit* circuit, const GateRec& g) {
+  if (!circuit) return NQPU_NULL_POINTER;
+  CircuitImpl* c = Cc(circuit);
+  const NqpuError e = check_rec(c, g);
+  if (e != NQPU_OK) return e;
   c->gates.push_back(g);
   c->version++;
   return NQPU_OK;
@@ -582,6 +588,38 @@ extern "C" NqpuError nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uin
   GateRec g = mk(G_CUSTOM2_FFI, qi(q1), qi(q2));
   for (int i = 0; i < 16; ++i) g.m[i] = cplx(matrix[i].re, matrix[i].im);
   return add_rec(c, g);
+}
+
+extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t* codes, const int32_t* qubits,
+                                            const double* params, const NqpuComplex* matrices, uint32_t count) {
+  if (!circuit) return NQPU_NULL_POINTER;
+  if (count == 0) return NQPU_OK;
+  if (!codes || !qubits || !params) return NQPU_NULL_POINTER;
+  CircuitImpl* c = Cc(circuit);
+  std::vector<GateRec> add;
+  try {
+    add.reserve(count);
+  } catch (...) {
+    return NQPU_ALLOCATION_FAILED;
+  }
+  for (uint32_t i = 0; i < count; ++i) {
+    if (codes[i] >= uint32_t(G_COUNT)) return NQPU_INVALID_PARAMETER;
+    GateRec g = mk(uint8_t(codes[i]), qubits[3 * i], qubits[3 * i + 1], qubits[3 * i + 2], params[4 * i],
+                   params[4 * i + 1], params[4 * i + 2], params[4 * i + 3]);
+    // unused qubit slots are ignored
+    for (int k = g.nq; k < 3; ++k) g.q[k] = 0;
+    if (g.code == G_CUSTOM1 || g.code == G_CUSTOM2_FFI || g.code == G_U2_LO) {
+      if (!matrices) return NQPU_NULL_POINTER;
+      const int nm = g.code == G_CUSTOM1 ? 4 : 16;
+      for (int k = 0; k < nm; ++k) g.m[k] = cplx(matrices[16 * i + k].re, matrices[16 * i + k].im);
+    }
+    const NqpuError e = check_rec(c, g);
+    if (e != NQPU_OK) return e;
+    add.push_back(g);
+  }
+  c->gates.insert(c->gates.end(), add.begin(), add.end());
+  c->version++;
+  return NQPU_OK;
 }
 
 extern "C" NqpuError nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode) {

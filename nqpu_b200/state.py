@@ -240,6 +240,29 @@ class Circuit:
         if gates:
             self.extend(gates)
 
+    @classmethod
+    def from_arrays(cls, num_qubits: int, codes, qubits, params, matrices=None) -> "Circuit":
+        """Circuit from flat arrays in one nqpu_circuit_add_gates call: codes [G]
+        (circuits.GATE_CODES), qubits [G, 3], params [G, 4], matrices [G, 16]
+        complex (custom gates only) or None."""
+        c = cls(num_qubits)
+        ca = np.ascontiguousarray(codes, dtype=np.uint32)
+        qa = np.ascontiguousarray(qubits, dtype=np.int32).reshape(-1, 3)
+        pa = np.ascontiguousarray(params, dtype=np.float64).reshape(-1, 4)
+        if not (len(ca) == len(qa) == len(pa)):
+            raise ValueError("codes, qubits and params differ in length")
+        ma = None
+        if matrices is not None:
+            ma = np.ascontiguousarray(matrices, dtype=np.complex128).reshape(-1, 16)
+            if len(ma) != len(ca):
+                raise ValueError("matrices differ in length")
+        mp = ma.ctypes.data_as(C.POINTER(NqpuComplex)) if ma is not None else None
+        check(c.lib.nqpu_circuit_add_gates(c.h_, ca.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           qa.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           pa.ctypes.data_as(C.POINTER(C.c_double)), mp, len(ca)),
+              "circuit_add_gates")
+        return c
+
     def close(self):
         if getattr(self, "h_", None):
             self.lib.nqpu_circuit_destroy(self.h_)
@@ -270,8 +293,51 @@ class Circuit:
         check(fn(self.h_, *qs, *ps), name)
 
     def extend(self, gates):
-        for g in gates:
-            self.add(g[0], g[1], g[2] if len(g) > 2 else (), g[3] if len(g) > 3 else None)
+        """Append a gate list with one nqpu_circuit_add_gates call."""
+        from .circuits import GATE_CODES
+        gates = gates if isinstance(gates, list) else list(gates)
+        m = len(gates)
+        if m == 0:
+            return
+        names = [g[0] for g in gates]
+        codes = np.fromiter(map(GATE_CODES.__getitem__, names), dtype=np.uint32, count=m)
+        qls = [g[1] for g in gates]
+        qlen = np.fromiter(map(len, qls), dtype=np.int64, count=m)
+        ar = np.fromiter((1 if n in MID_GATES else ARITY[n] for n in names), dtype=np.int64, count=m)
+        bad = np.nonzero(qlen != ar)[0]
+        if bad.size:
+            i = int(bad[0])
+            raise ValueError(f"{names[i]} takes {ar[i]} qubits")
+        qa = np.zeros((m, 3), dtype=np.int32)
+        for k in (1, 2, 3):
+            idx = np.nonzero(ar == k)[0]
+            if idx.size:
+                qa[idx, :k] = np.array([qls[i] for i in idx], dtype=np.int64).reshape(-1, k)
+        npar = np.fromiter(map(NPARAMS.__getitem__, names), dtype=np.int64, count=m)
+        pa = np.zeros((m, 4), dtype=np.float64)
+        for k in (1, 2, 3, 4):
+            idx = np.nonzero(npar == k)[0]
+            if idx.size:
+                rows = [tuple(gates[i][2])[:k] if len(gates[i]) > 2 else () for i in idx]
+                if any(len(r) != k for r in rows):
+                    j = int(idx[[len(r) != k for r in rows].index(True)])
+                    raise ValueError(f"{names[j]} takes {k} parameters")
+                pa[idx, :k] = np.array(rows, dtype=np.float64)
+        mats = None
+        cidx = np.nonzero(np.isin(codes, [GATE_CODES["custom1"], GATE_CODES["custom2"], GATE_CODES["u2lo"]]))[0]
+        if cidx.size:
+            mats = np.zeros((m, 16), dtype=np.complex128)
+            for i in cidx:
+                mm = np.asarray(gates[i][3], dtype=np.complex128).reshape(-1)
+                want = 4 if names[i] == "custom1" else 16
+                if mm.size != want:
+                    raise ValueError(f"{names[i]} takes a {'2x2' if want == 4 else '4x4'} matrix")
+                mats[i, :want] = mm
+        mp = mats.ctypes.data_as(C.POINTER(NqpuComplex)) if mats is not None else None
+        check(self.lib.nqpu_circuit_add_gates(self.h_, codes.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                              qa.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              pa.ctypes.data_as(C.POINTER(C.c_double)), mp, m),
+              "circuit_add_gates")
 
     def execute(self, state: StateVector, mode: str = "tiled"):
         check(self.lib.nqpu_circuit_execute_ex(self.h_, state.h_, MODES[mode]), "circuit_execute")
