@@ -109,6 +109,33 @@ def cpu_reference_rate(gates, n, f32, budget_s, threads=0):
     return done / el, done, el, O.max_threads()
 
 
+def cpu_circuit_rate(items, budget_s, read):
+    """Oracle circuits/s over a stride sample of (n, gates) items: circuits are
+    taken at a fixed stride through the list (every size class appears) and run
+    one by one, gates then the read-out `read(state, k)`, until `budget_s`; a
+    circuit cut off by the budget counts by the fraction of its gates done."""
+    from oracle import oracle as O
+    stride = max(1, len(items) // 64)
+    order = [i for s0 in range(stride) for i in range(s0, len(items), stride)]
+    done, t0 = 0.0, time.perf_counter()
+    for i in order:
+        if time.perf_counter() - t0 >= budget_s:
+            break
+        n, gates = items[i]
+        st = O.OracleState(n, f32=True)
+        g = 0
+        while g < len(gates) and time.perf_counter() - t0 < budget_s:
+            st.apply(gates[g:g + 8])
+            g += 8
+        if g < len(gates):
+            done += g / len(gates)
+            break
+        read(st, i)
+        done += 1
+    el = time.perf_counter() - t0
+    return done / el, done, el, O.max_threads(), stride
+
+
 def run_reference(args):
     from nqpu_b200.circuits import brickwork
     rank = int(os.environ.get("RANK", "0"))
@@ -386,7 +413,15 @@ def run_precision(args):
     w = StateVector(n, "c64")
     c.execute(w, "fused")
     w.close()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
     sv64, rec64, l64 = run("c64", "fused")
+    clk = clocks.stop()
     sv128, rec128, l128 = run("c128", "tiled")
     f = sv64.fidelity(sv128)
     errs = [{"step": every * (i + 1), "max_abs_dZ": float(np.abs(a[0] - b[0]).max()), "abs_dZ0Z1": abs(a[1] - b[1])}
@@ -404,9 +439,41 @@ def run_precision(args):
     fused_ms = sum(l64)
     G = len(chunk) * (steps // every)
     st = c.plan_stats(n, "c64", "fused")
+    # e2e through the public API: gate list -> circuit -> fused runs with the
+    # <Z_i> and <Z0 Z1> read-outs on the host, wall clock
+    e2e = None
+    if not args.quick:
+        t0 = time.perf_counter()
+        ce = Circuit(n, chunk)
+        se = StateVector(n, "c64")
+        se.set_basis(neel_index(n))
+        for _ in range(steps // every):
+            ce.execute(se, "fused")
+            se.expectation_z_all()
+            se.expectation_pauli_string(zz)
+        et = time.perf_counter() - t0
+        se.close()
+        ce.close()
+        e2e = {"value": G / et, "unit": "gates/s", "h2d_bytes_per_step": int(st.get("upload_bytes", 0)),
+               "d2h_bytes_per_step": (8 * n + 8) * (steps // every), "seconds_per_step": et,
+               "timing": "host wall clock: circuit from the gate list, state init, fused runs (plan build and "
+                         "B-operand upload included) and the read-outs every 10 steps"}
+    # CPU baseline: the oracle's per-gate passes on the same TFIM chunk at a
+    # size whose complex64 state fits host memory comfortably (26 qubits),
+    # scaled to 32 qubits by the state size (each pass is linear in 2^n)
+    cpu = None
+    if not args.quick and not args.no_cpu:
+        nc = min(n, 26)
+        cg, _ = tfim_trotter(nc, every, seed=args.seed)
+        rate, done, el, cores = cpu_reference_rate(cg, nc, True, args.cpu_budget_s)
+        cpu = {"value": rate / (1 << (n - nc)), "unit": "gates/s", "cores": cores, "kind": "port",
+               "sample": f"first {done} gates of the {nc}-qubit TFIM chunk in {el:.1f} s ({rate:.1f} gates/s), "
+                         f"scaled by 2^{nc - n} to {n} qubits"}
     line = {
-        "form": "precision", "metric": "gates/s (32q TFIM Trotter, fused split-TF32 tensor cores)",
-        "value": G / (fused_ms / 1000), "unit": "gates/s", "dtype": "c64", "data": "synthetic",
+        "form": "precision", "metric": f"gates/s ({n}q TFIM Trotter, fused split-TF32 tensor cores)",
+        "value": G / (fused_ms / 1000), "unit": "gates/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": fused_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64", "data": "synthetic",
         "config": {"workload": f"TFIM {n}q {steps} Trotter steps dt 0.05, Neel start", "gates": G,
                    "fused_unitaries": st["passes"] * (steps // every), "seed": args.seed},
         "seconds": fused_ms / 1000,
@@ -418,6 +485,7 @@ def run_precision(args):
                              "max_abs_dZ": max(e["max_abs_dZ"] for e in errs),
                              "max_abs_dZ0Z1": max(e["abs_dZ0Z1"] for e in errs)},
         "fp64_reference_seconds": sum(l128) / 1000, "plain_tiled_c64": plain,
+        "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": len(l64), "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
@@ -543,6 +611,20 @@ def run_batch(args):
         for c in cs:
             c.close()
 
+    cpu = None
+    if not args.quick and not args.no_cpu:
+        def read_h(st, i):
+            _, _, J, h = items[i]
+            n = len(h)
+            z = [st.pauli_string("I" * q + "ZZ" + "I" * (n - q - 2)) for q in range(n - 1)]
+            x = [st.pauli_string("I" * q + "X" + "I" * (n - q - 1)) for q in range(n)]
+            return float(np.dot(J, z) + np.dot(h, x))
+        rate, done, el, cores, stride = cpu_circuit_rate([(n, g) for n, g, _, _ in items], args.cpu_budget_s,
+                                                         read_h)
+        cpu = {"value": rate, "unit": "circuits/s", "cores": cores, "kind": "port",
+               "sample": f"{done:.2f} of the {count} circuits (stride {stride}, every size class) in {el:.1f} s: "
+                         f"per-gate passes and the Ising <H> Pauli terms"}
+
     line = {
         "form": "batch", "metric": f"circuits/s ({count} mixed-size HEA circuits, <H> per circuit)",
         "value": value, "unit": "circuits/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
@@ -566,7 +648,7 @@ def run_batch(args):
         "accuracy": {"max_rel_err_vs_fp64": err_fp64, "max_rel_err_vs_plain_c64": err_plain,
                      "tolerance": "|<H> - <H>_FP64| <= 1e-5 * (sum|J| + sum|h|)"},
         "host_build_s": host_build_s, "prepare_s": prepare_s, "wall_s_timed": wall,
-        "e2e": e2e, "gpu_launches": steps, "clocks": clk,
+        "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": steps, "clocks": clk,
     }
     print(json.dumps(line), flush=True)
     b.close()
@@ -592,8 +674,13 @@ def run_serve(args):
     circs = [Circuit(r["n"], brickwork(r["n"], r["depth"], r["seed"])) for r in base]
     build_s = time.perf_counter() - t0
     G = sum(c.gate_count for c in circs)
-    passes = [c.plan_stats(r["n"], "c64", "tiled")["passes"] if r["n"] >= 5 else c.gate_count
-              for c, r in zip(circs, base)]
+    pstats = [c.plan_stats(r["n"], "c64", "tiled") for c, r in zip(circs, base)]
+    passes = [p_["passes"] for p_ in pstats]
+    # bytes each rate step moves: every request's plan tables (and its shot
+    # uniforms) host->device, its <Z_i> or outcomes device->host
+    h2d_step = sum(int(p_.get("upload_bytes", 0)) + (1024 * 8 if r["kind"] == "shots" else 0)
+                   for p_, r in zip(pstats, base))
+    d2h_step = sum(8 * r["n"] if r["kind"] == "zall" else 1024 * 8 for r in base)
     launches = sum(1 + p + (2 if r["kind"] == "zall" else 3) for p, r in zip(passes, base))
     budget = int(args.serve_budget_gb * (1 << 30))
     rates = [float(x) for x in args.rates.split(",")]
@@ -676,6 +763,19 @@ def run_serve(args):
     svc = np.array(svc)
     plain_rate = 1.0 / svc.mean()
     top = sweep[-1]
+    cpu = None
+    if not args.quick and not args.no_cpu:
+        from oracle import oracle as O
+        def read_req(st, i):
+            r = base[i]
+            if r["kind"] == "zall":
+                return st.expectation_z_all()
+            return st.sample_uniforms(O.xorshift_uniforms(r["seed"], 1024))
+        reqs = [(r["n"], brickwork(r["n"], r["depth"], r["seed"])) for r in base]
+        rate, done, el, cores, stride = cpu_circuit_rate(reqs, args.cpu_budget_s, read_req)
+        cpu = {"value": rate, "unit": "circuits/s", "cores": cores, "kind": "port",
+               "sample": f"{done:.2f} of the {count} requests (stride {stride}) one after another in {el:.1f} s: "
+                         f"per-gate passes, then all <Z_i> or 1024 shots"}
     line = {
         "form": "serve", "metric": "served circuits/s at the highest offered rate (p50/p99 latency beside it)",
         "value": top["circuits_per_s"], "unit": "circuits/s", "n_gpus": 1, "steps": len(rates), "warmup": 4,
@@ -697,10 +797,10 @@ def run_serve(args):
         "results_identical_across_rates": same,
         "host_circuit_build_s": build_s,
         "e2e": {"value": top["circuits_per_s"], "unit": "circuits/s",
-                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "h2d_bytes_per_step": h2d_step, "d2h_bytes_per_step": d2h_step,
                 "timing": "host wall clock from first submit to last result; each request's plan tables and "
                           "uniforms go host->device, its <Z_i> or outcomes device->host, inside the span"},
-        "gpu_launches": launches * len(rates), "clocks": clk,
+        "cpu_baseline": cpu, "gpu_launches": launches * len(rates), "clocks": clk,
     }
     print(json.dumps(line), flush=True)
     for c in circs:
