@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       const uint32_t nvec = 1u << (P.k - 1);
       init_tile(nvec, true);
       __syncthreads();
-      run_tile_stages<float>(sv, P, tabs, ops, 0u);
+      run_tile_stages<float, true>(sv, P, tabs, ops, 0u);
       double jtot;
       load_obs(C, &jtot);
       __syncthreads();
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         cp_async_wait0();
       }
       __syncthreads();
-      run_tile_stages<float>(sv, P, tabs, ops, ext);
+      run_tile_stages<float, true>(sv, P, tabs, ops, ext);
       for (uint32_t u = tid; u < nvec; u += blockDim.x) {
         const uint32_t t = u << 1;
         const uint64_t g = base + (t & lowmask) + hi_off[t >> c];

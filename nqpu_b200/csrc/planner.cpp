@@ -275,6 +275,16 @@ static TileOp<Real> encode_op(const Op& o, const int* tile_pos, const int* reg_o
     }
     t.fast = uint8_t(8 + 8 * t.rb0 + v);
   }
+  // Diagonal shapes (read by the batch executor, whose HEA circuits are two
+  // thirds diagonal ops; d = register bit, nrb for a thread-level bit):
+  //   48 + d           diag(d0, d1) on bit d, no controls
+  //   128 + creg       phase on register mask creg (controls outside the registers: tc)
+  //   160 + 8 d0 + d1  diagonal on bits (d0, d1), no controls
+  const int nrb = sizeof(Real) == 4 ? 5 : 4;
+  auto dbit = [&](uint8_t d) { return d == 0xFF ? nrb : int(d); };
+  if (o.kind == OP_D1 && t.creg == 0 && t.cnr == 0) t.fast2 = uint8_t(48 + dbit(t.dreg0));
+  if (o.kind == OP_PH) t.fast2 = uint8_t(128 + t.creg);
+  if (o.kind == OP_D2 && t.creg == 0 && t.cnr == 0) t.fast2 = uint8_t(160 + 8 * dbit(t.dreg0) + dbit(t.dreg1));
   return t;
 }
 

@@ -133,7 +133,7 @@ struct TileOp {
   uint8_t creg;         // mask over register bits: controls held in registers
   uint8_t dreg0, dreg1; // register bit of diagonal qubit 0/1, 0xFF when not a register bit
   uint8_t fast;         // flat dispatch code of the common cases (0: decode the fields)
-  uint8_t pad0;
+  uint8_t fast2;        // flat dispatch code of the diagonal shapes (read by the batch executor)
   uint32_t cnr;         // virtual-index mask of controls not in registers
   uint32_t dv0, dv1;    // virtual-index mask of diagonal qubit 0/1 when not a register bit
   uint32_t pad1[3];     // header is 32 B so m[] is 16-byte aligned

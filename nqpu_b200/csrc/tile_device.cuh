@@ -308,7 +308,7 @@ __device__ __forceinline__ void dispatch_sw_b(C (&a)[NA], int b1, bool tc, uint3
 
 // Apply ops [ob, oe) of a stage to the thread's register block.
 // vbase = virtual index of register amplitude 0 (register bits are zero in it).
-template <typename Real, int NA, int NRB>
+template <typename Real, int NA, int NRB, bool kDiagFlat = false>
 __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
                                                 const TileOp<Real>* __restrict__ ops, int ob,
                                                 int oe, uint32_t vbase) {
@@ -361,6 +361,43 @@ __device__ __forceinline__ void apply_stage_ops(typename Tr<Real>::C (&a)[NA],
         default: break;
       }
       continue;
+    }
+    // the batch executor's variant also takes the diagonal shapes through a
+    // flat switch (TileOp::fast2); measured +1 % there, while the tiled pass
+    // kernel ran QFT passes 1 % slower with it
+    if constexpr (kDiagFlat) {
+      const uint32_t fast2 = (h0.y >> 24) & 0xFF;
+      if (fast2 != 0) {
+        switch (fast2) {
+#define NQ_FD1(B) case 48 + B: \
+          if constexpr (B <= NRB) rb_d1<C, NA, B, NRB>(a, pm0, pm1, (vbase & dv0) ? 1u : 0u); \
+          break;
+          NQ_FD1(0) NQ_FD1(1) NQ_FD1(2) NQ_FD1(3) NQ_FD1(4) NQ_FD1(5)
+#undef NQ_FD1
+#define NQ_FPH(V) case 128 + V: \
+          if constexpr (V < (1 << NRB)) { \
+            if (tc) rb_ph<C, NA, V>(a, pm0, (pm0.x == Real(-1)) && (pm0.y == Real(0))); \
+          } \
+          break;
+          NQ_FPH(0) NQ_FPH(1) NQ_FPH(2) NQ_FPH(3) NQ_FPH(4) NQ_FPH(5) NQ_FPH(6) NQ_FPH(7)
+          NQ_FPH(8) NQ_FPH(9) NQ_FPH(10) NQ_FPH(11) NQ_FPH(12) NQ_FPH(13) NQ_FPH(14) NQ_FPH(15)
+          NQ_FPH(16) NQ_FPH(17) NQ_FPH(18) NQ_FPH(19) NQ_FPH(20) NQ_FPH(21) NQ_FPH(22) NQ_FPH(23)
+          NQ_FPH(24) NQ_FPH(25) NQ_FPH(26) NQ_FPH(27) NQ_FPH(28) NQ_FPH(29) NQ_FPH(30) NQ_FPH(31)
+#undef NQ_FPH
+#define NQ_FD2V(D0, D1) case 160 + 8 * D0 + D1: \
+          if constexpr (D0 <= NRB && D1 <= NRB && (D0 != D1 || D0 == NRB)) { \
+            const C m[4] = {pm0, pm1, pm2, pm3}; \
+            rb_d2<C, NA, D0, D1, NRB>(a, m, (vbase & dv0) ? 1u : 0u, (vbase & dv1) ? 1u : 0u); \
+          } \
+          break;
+#define NQ_FD2(D0) NQ_FD2V(D0, 0) NQ_FD2V(D0, 1) NQ_FD2V(D0, 2) NQ_FD2V(D0, 3) NQ_FD2V(D0, 4) NQ_FD2V(D0, 5)
+          NQ_FD2(0) NQ_FD2(1) NQ_FD2(2) NQ_FD2(3) NQ_FD2(4) NQ_FD2(5)
+#undef NQ_FD2
+#undef NQ_FD2V
+          default: break;
+        }
+        continue;
+      }
     }
     switch (kind) {
       case OP_U1: {
@@ -602,7 +639,7 @@ __device__ __forceinline__ void build_pass_tabs(const PassRec& P, const StageRec
 // memory `sv` (swizzled vector slots), with the pass's stage tables in `tabs`.
 // Every thread of the CTA must call it (it contains block barriers); threads
 // >= nvec/16 only take part in them.
-template <typename Real>
+template <typename Real, bool kDiagFlat = false>
 __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict__ sv, const PassRec& P,
                                                 const uint32_t* __restrict__ tabs,
                                                 const TileOp<Real>* __restrict__ ops, uint32_t ext) {
@@ -632,7 +669,7 @@ __device__ __forceinline__ void run_tile_stages(typename Tr<Real>::V* __restrict
         unpack_vec<Real>(sv[slot], a + r * APV);
       }
       const uint32_t vbase = (ub << VB) | ext;
-      apply_stage_ops<Real, NA, NRB>(a, ops, int(Tb[StageTab::OB]), int(Tb[StageTab::OE]), vbase);
+      apply_stage_ops<Real, NA, NRB, kDiagFlat>(a, ops, int(Tb[StageTab::OB]), int(Tb[StageTab::OE]), vbase);
       // Write-back through the stage's deferred permutation pi(p) = A p ^ w:
       // register amplitude p goes to the slot of logical index pi(p).  Slot
       // offsets are linear in the free register bits (register bits
