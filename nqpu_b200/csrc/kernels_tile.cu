@@ -158,10 +158,14 @@ cudaError_t launch_tile_pass_cfg(Real* amp, const PassRec& host_pass, const Pass
     return cudaErrorInvalidValue;
   auto kern = k_tile_pass<Real, KMAX, MINB>;
   constexpr int kThreads = (1 << (KMAX - Tr<Real>::kVecBit)) / kVecPerThread;
-  const size_t smem = tile_smem_bytes<Real, KMAX>(MINB);
+  // shared memory of this launch: the tile buffer(s), the high-offset table and
+  // the stage tables of this pass only (more CTAs fit when passes are short)
+  const size_t smem_max = tile_smem_bytes<Real, KMAX>(MINB);
+  const size_t smem = smem_max - sizeof(uint32_t) * kStageTabWords *
+                                     size_t(kMaxPassStages - (host_pass.stage_end - host_pass.stage_begin));
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
     if (e != cudaSuccess) return e;
     configured = true;
   }
