@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   }
   if (warp == 0) {
     const uint32_t holder = static_cast<uint32_t>(__cvta_generic_to_shared(&tmem_holder));
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(holder), "r"(64));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(holder), "r"(128));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -277,14 +277,13 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     *reinterpret_cast<float4*>(a_lo + o0) =
         make_float4(tf32_rn(x.x - h.x), tf32_rn(x.y - h.y), tf32_rn(x.z - h.z), tf32_rn(x.w - h.w));
   };
-  // software pipeline: the next tile's HBM loads are in flight while the
-  // current tile's MMAs, epilogue and stores run
+  // Software pipeline over this CTA's tiles t0, t1, ... (two accumulators of
+  // 64 TMEM columns): the split of tile t+1 into the operand planes waits only
+  // for the MMAs of tile t; the MMAs of tile t+1 then run while the epilogue
+  // of tile t drains the other accumulator; the HBM loads of tile t+2 are in
+  // flight meanwhile and the tiles after it are prefetched into L2.
   float4 v[kLoadSteps];
-  if (uint64_t(blockIdx.x) < n_tiles) load_tile(tile_base_of(blockIdx.x), v);
-  if (uint64_t(blockIdx.x) + gridDim.x < n_tiles) prefetch_tile(tile_base_of(blockIdx.x + gridDim.x));
-  if (uint64_t(blockIdx.x) + 2ull * gridDim.x < n_tiles) prefetch_tile(tile_base_of(blockIdx.x + 2ull * gridDim.x));
-  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    const uint64_t tb = tile_base_of(tile);
+  auto put_tile = [&]() {
     if (A.lane_over_j) {
 #pragma unroll
       for (int i = 0; i < kLoadSteps; ++i) put2(op_t ^ it_op[(uint32_t(i) + g) & 7u], v[i]);
@@ -300,44 +299,46 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-
+  };
+  auto issue_mma = [&](uint32_t acc_col) {
     if (tid == 0) {
       uint32_t acc = 0;
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk) {
         const uint32_t off = (kk >> 2) * kAtomBytes + (kk & 3) * 32;
         const uint32_t boff = (kk >> 2) * (64 * 128) + (kk & 3) * 32;
-        mma_tf32(tmem, umma_desc(ahi_s + off), umma_desc(bhi_s + boff), acc);
+        mma_tf32(tmem + acc_col, umma_desc(ahi_s + off), umma_desc(bhi_s + boff), acc);
         acc = 1;
-        mma_tf32(tmem, umma_desc(ahi_s + off), umma_desc(blo_s + boff), 1);
-        mma_tf32(tmem, umma_desc(alo_s + off), umma_desc(bhi_s + boff), 1);
+        mma_tf32(tmem + acc_col, umma_desc(ahi_s + off), umma_desc(blo_s + boff), 1);
+        mma_tf32(tmem + acc_col, umma_desc(alo_s + off), umma_desc(bhi_s + boff), 1);
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_addr)
                    : "memory");
     }
-    if (tile + gridDim.x < n_tiles) load_tile(tile_base_of(tile + gridDim.x), v);
-    if (tile + 3ull * gridDim.x < n_tiles) prefetch_tile(tile_base_of(tile + 3ull * gridDim.x));
-    // bounded wait for the MMAs
-    {
-      uint32_t it = 0;
-      bool done = false;
-      while (!(done = mbar_try_wait(mbar_addr, phase)) && ++it < kWaitLimit) {
-      }
-      if (!done) {
-        atomicExch(err, 1);
-        abort_flag = 1;
-      }
+  };
+  // bounded wait for the last MMAs issued; false: the CTA gives up (error flagged)
+  auto wait_mma = [&]() {
+    uint32_t it = 0;
+    bool done = false;
+    while (!(done = mbar_try_wait(mbar_addr, phase)) && ++it < kWaitLimit) {
     }
+    if (!done) {
+      atomicExch(err, 1);
+      abort_flag = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
-    if (abort_flag) break;
-    phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-
-    // TMEM -> registers: warp w reads lanes 32 (w % 4) .. + 31 (row = tid % 128)
-    // and the fp32 columns 32 (w / 4) .. + 31 (complex columns 16 (w / 4) .. + 15)
+    phase ^= 1u;
+    return abort_flag == 0;
+  };
+  // accumulator at column acc_col -> HBM, rows straight from TMEM: warp w reads
+  // lanes 32 (w % 4) .. + 31 (row = tid % 128) and the fp32 columns
+  // 32 (w / 4) .. + 31 of the accumulator (complex columns 16 (w / 4) .. + 15)
+  auto epilogue = [&](uint64_t tb, uint32_t acc_col) {
     uint32_t r[32];
-    const uint32_t row = uint32_t(tid) & 127u, jb = uint32_t(warp >> 2) * 16u;
-    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + 2u * jb;
+    const uint32_t jb = uint32_t(warp >> 2) * 16u;
+    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + acc_col + 2u * jb;
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -348,9 +349,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-
-    // row of D -> HBM directly: the warp's 32 rows are the thread rows; when
-    // qubit 0 is fused, columns (j, j + 1) are adjacent amplitudes (16 bytes)
+    // when qubit 0 is fused, columns (j, j + 1) are adjacent amplitudes (16 bytes)
     double tile_norm = 0.0;
     float2* out = reinterpret_cast<float2*>(amp) + tb + row_addr;
     if (A.lane_over_j) {
@@ -371,8 +370,33 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
       }
     }
     norm_acc += tile_norm;
-    // TMEM is read and the MMAs are complete: the next tile's operand split
-    // may start; the barrier after it orders these reads before the next MMAs
+  };
+  const uint64_t G = gridDim.x;
+  uint64_t tile = blockIdx.x;
+  if (tile < n_tiles) {
+    load_tile(tile_base_of(tile), v);
+    if (tile + G < n_tiles) prefetch_tile(tile_base_of(tile + G));
+    if (tile + 2 * G < n_tiles) prefetch_tile(tile_base_of(tile + 2 * G));
+    put_tile();
+    issue_mma(0);
+    if (tile + G < n_tiles) load_tile(tile_base_of(tile + G), v);
+    if (tile + 3 * G < n_tiles) prefetch_tile(tile_base_of(tile + 3 * G));
+    uint32_t cur = 0;  // TMEM column of the accumulator that holds `tile`
+    bool ok = wait_mma();
+    while (ok) {
+      const uint64_t next = tile + G;
+      if (next < n_tiles) {
+        put_tile();  // tile `next`: the operand planes are free (its predecessor's MMAs are done)
+        issue_mma(cur ^ 64u);
+        if (next + G < n_tiles) load_tile(tile_base_of(next + G), v);
+        if (next + 3 * G < n_tiles) prefetch_tile(tile_base_of(next + 3 * G));
+      }
+      epilogue(tile_base_of(tile), cur);
+      if (next >= n_tiles) break;
+      ok = wait_mma();  // also orders this epilogue's TMEM reads before the next MMAs into `cur`
+      tile = next;
+      cur ^= 64u;
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   // per-CTA FP64 norm partial (fixed-order tree: warp shuffles, then warp 0)
@@ -388,7 +412,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     for (int w = 0; w < kFusedThreads / 32; ++w) t += wsum[w];
     out_norm[blockIdx.x] = t;
   }
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(128));
 }
 
 // ---------------------------------------------------------------------------
