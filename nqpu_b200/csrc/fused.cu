@@ -48,10 +48,14 @@ namespace nqpu {
 // ---------------------------------------------------------------------------
 // Device kernel
 // ---------------------------------------------------------------------------
-constexpr int kFusedThreads = 256;         // two threads per group row (M = 128): column halves
-constexpr int kTidBits = 8;                // log2(kFusedThreads)
-constexpr int kLoadSteps = 4096 / (2 * kFusedThreads);  // 16-byte loads per thread per tile
-static_assert((1 << kTidBits) == kFusedThreads && kLoadSteps == 8, "fused tile decomposition");
+// Eight warps with two roles: warps 0-3 load tiles from HBM and split them
+// into the operand planes, warps 4-7 drain the accumulators (one group row
+// per thread, TMEM lane = row) to HBM.
+constexpr int kFusedThreads = 256;
+constexpr int kProdThreads = 128;          // warps 0-3
+constexpr int kTidBits = 7;                // log2(kProdThreads)
+constexpr int kLoadSteps = 4096 / (2 * kProdThreads);  // 16-byte loads per loading thread per tile
+static_assert((1 << kTidBits) == kProdThreads && kLoadSteps == 16, "fused tile decomposition");
 constexpr int kAtomBytes = 128 * 128;      // one K-atom (32 tf32) of 128 rows
 constexpr int kAPlane = 2 * kAtomBytes;    // 32 KB: 128 rows x 64 tf32
 constexpr int kBPlane = 2 * 64 * 128;      // 16 KB: 64 rows x 64 tf32
@@ -160,7 +164,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   const uint32_t mbar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar));
 
   // Sub-cube index u = h | tid << 1 | i << (1 + kTidBits) (h: amplitude in a
-  // 16-byte pair, i: load step).  Global offset, row and column of u are XORs of the parts.
+  // 16-byte pair, tid: loading thread, i: load step).  Global offset, row and column of u are XORs of the parts.
   auto part = [&](uint32_t u, uint64_t* addr, uint32_t* row, uint32_t* col) {
     uint64_t a = 0;
     uint32_t r = 0, c = 0;
@@ -176,7 +180,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   };
   // The swizzled operand offset sw128_off(r, 2c) is GF(2)-linear in the bits
   // of (r, c) (its fields occupy disjoint bits), so the offset of sub-cube
-  // index u = h | tid << 1 | step << 9 is the XOR of the offsets of its parts.
+  // index u = h | tid << 1 | step << 8 is the XOR of the offsets of its parts.
   auto op_off = [&](uint32_t r, uint32_t c) { return sw128_off<128>(r, 2 * c); };
   if (tid < kLoadSteps) {
     uint64_t a;
@@ -193,11 +197,12 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   }
   // load-step rotation by lane group (8 lanes = 128 contiguous bytes stay together)
   const uint32_t g = A.rot ? uint32_t((lane >> 3) & 3) : 0u;
+  const bool loader = tid < kProdThreads;
   uint64_t t_addr;
   uint32_t t_row, t_col, h_row, h_col;
   {
     uint64_t a;
-    part(uint32_t(tid) << 1, &t_addr, &t_row, &t_col);
+    part(uint32_t(tid & (kProdThreads - 1)) << 1, &t_addr, &t_row, &t_col);
     part(1u, &a, &h_row, &h_col);
   }
   const uint32_t op_t = op_off(t_row, t_col), op_h = op_off(h_row, h_col);
@@ -252,7 +257,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   auto load_tile = [&](uint64_t tb, float4 (&v)[kLoadSteps]) {
     const float4* src4 = reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(amp) + tb + t_addr);
 #pragma unroll
-    for (int i = 0; i < kLoadSteps; ++i) v[i] = __ldcs(src4 + (it_addr[(uint32_t(i) + g) & 7u] >> 1));
+    for (int i = 0; i < kLoadSteps; ++i) v[i] = __ldcs(src4 + (it_addr[(uint32_t(i) + g) & 15u] >> 1));
   };
   // the tiles two and three ahead are pulled into L2 meanwhile (no registers
   // or shared memory held), so the next loads meet L2 rather than DRAM latency
@@ -260,7 +265,7 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     const float4* src4 = reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(amp) + tb + t_addr);
 #pragma unroll
     for (int i = 0; i < kLoadSteps; ++i)
-      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(src4 + (it_addr[(uint32_t(i) + g) & 7u] >> 1)));
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(src4 + (it_addr[(uint32_t(i) + g) & 15u] >> 1)));
   };
   // HBM -> A_hi / A_lo (split), swizzled K-major rows; (re, im) = columns
   // (2j, 2j + 1) share one aligned 8-byte slot of a 16-byte chunk
@@ -278,27 +283,27 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
         make_float4(tf32_rn(x.x - h.x), tf32_rn(x.y - h.y), tf32_rn(x.z - h.z), tf32_rn(x.w - h.w));
   };
   // Software pipeline over this CTA's tiles t0, t1, ... (two accumulators of
-  // 64 TMEM columns): the split of tile t+1 into the operand planes waits only
-  // for the MMAs of tile t; the MMAs of tile t+1 then run while the epilogue
-  // of tile t drains the other accumulator; the HBM loads of tile t+2 are in
-  // flight meanwhile and the tiles after it are prefetched into L2.
+  // 64 TMEM columns).  While the epilogue warps drain tile t from one
+  // accumulator, the loading warps split tile t+1 (loaded during the previous
+  // round) into the operand planes, which the MMAs of tile t have released,
+  // and issue its MMAs into the other accumulator; the HBM loads of tile t+2
+  // follow, and the tiles after it are prefetched into L2.
   float4 v[kLoadSteps];
+  // loading warps: operand split of the tile in v (writers make their shared
+  // stores visible to the tensor core before the barrier)
   auto put_tile = [&]() {
     if (A.lane_over_j) {
 #pragma unroll
-      for (int i = 0; i < kLoadSteps; ++i) put2(op_t ^ it_op[(uint32_t(i) + g) & 7u], v[i]);
+      for (int i = 0; i < kLoadSteps; ++i) put2(op_t ^ it_op[(uint32_t(i) + g) & 15u], v[i]);
     } else {
 #pragma unroll
       for (int i = 0; i < kLoadSteps; ++i) {
-        const uint32_t o0 = op_t ^ it_op[(uint32_t(i) + g) & 7u];
+        const uint32_t o0 = op_t ^ it_op[(uint32_t(i) + g) & 15u];
         put(o0, v[i].x, v[i].y);
         put(o0 ^ op_h, v[i].z, v[i].w);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   };
   auto issue_mma = [&](uint32_t acc_col) {
     if (tid == 0) {
@@ -332,41 +337,44 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     phase ^= 1u;
     return abort_flag == 0;
   };
-  // accumulator at column acc_col -> HBM, rows straight from TMEM: warp w reads
-  // lanes 32 (w % 4) .. + 31 (row = tid % 128) and the fp32 columns
-  // 32 (w / 4) .. + 31 of the accumulator (complex columns 16 (w / 4) .. + 15)
+  // epilogue warps: accumulator at column acc_col -> HBM; warp w reads lanes
+  // 32 (w % 4) .. + 31 (row = tid % 128), all 64 fp32 columns in two halves
   auto epilogue = [&](uint64_t tb, uint32_t acc_col) {
-    uint32_t r[32];
-    const uint32_t jb = uint32_t(warp >> 2) * 16u;
-    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + acc_col + 2u * jb;
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    // when qubit 0 is fused, columns (j, j + 1) are adjacent amplitudes (16 bytes)
     double tile_norm = 0.0;
     float2* out = reinterpret_cast<float2*>(amp) + tb + row_addr;
-    if (A.lane_over_j) {
 #pragma unroll
-      for (int jj = 0; jj < 16; jj += 2) {
-        const float4 o = make_float4(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale,
-                                     __uint_as_float(r[2 * jj + 2]) * scale, __uint_as_float(r[2 * jj + 3]) * scale);
-        tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y) + double(o.z) * double(o.z) +
-                     double(o.w) * double(o.w);
-        __stcs(reinterpret_cast<float4*>(out + ctab[jb + uint32_t(jj)]), o);
-      }
-    } else {
+    for (int half = 0; half < 2; ++half) {
+      uint32_t r[32];
+      const uint32_t jb = uint32_t(half) * 16u;
+      const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + acc_col + 2u * jb;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      // when qubit 0 is fused, columns (j, j + 1) are adjacent amplitudes (16 bytes)
+      if (A.lane_over_j) {
 #pragma unroll
-      for (int jj = 0; jj < 16; ++jj) {
-        const float2 o = make_float2(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale);
-        tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
-        __stcs(out + ctab[jb + uint32_t(jj)], o);
+        for (int jj = 0; jj < 16; jj += 2) {
+          const float4 o = make_float4(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale,
+                                       __uint_as_float(r[2 * jj + 2]) * scale,
+                                       __uint_as_float(r[2 * jj + 3]) * scale);
+          tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y) + double(o.z) * double(o.z) +
+                       double(o.w) * double(o.w);
+          __stcs(reinterpret_cast<float4*>(out + ctab[jb + uint32_t(jj)]), o);
+        }
+      } else {
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          const float2 o = make_float2(__uint_as_float(r[2 * jj]) * scale, __uint_as_float(r[2 * jj + 1]) * scale);
+          tile_norm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+          __stcs(out + ctab[jb + uint32_t(jj)], o);
+        }
       }
     }
     norm_acc += tile_norm;
@@ -374,26 +382,41 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
   const uint64_t G = gridDim.x;
   uint64_t tile = blockIdx.x;
   if (tile < n_tiles) {
-    load_tile(tile_base_of(tile), v);
-    if (tile + G < n_tiles) prefetch_tile(tile_base_of(tile + G));
-    if (tile + 2 * G < n_tiles) prefetch_tile(tile_base_of(tile + 2 * G));
-    put_tile();
+    if (loader) {
+      load_tile(tile_base_of(tile), v);
+      if (tile + G < n_tiles) prefetch_tile(tile_base_of(tile + G));
+      if (tile + 2 * G < n_tiles) prefetch_tile(tile_base_of(tile + 2 * G));
+      put_tile();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     issue_mma(0);
-    if (tile + G < n_tiles) load_tile(tile_base_of(tile + G), v);
-    if (tile + 3 * G < n_tiles) prefetch_tile(tile_base_of(tile + 3 * G));
+    if (loader) {
+      if (tile + G < n_tiles) load_tile(tile_base_of(tile + G), v);
+      if (tile + 3 * G < n_tiles) prefetch_tile(tile_base_of(tile + 3 * G));
+    }
     uint32_t cur = 0;  // TMEM column of the accumulator that holds `tile`
     bool ok = wait_mma();
     while (ok) {
       const uint64_t next = tile + G;
-      if (next < n_tiles) {
-        put_tile();  // tile `next`: the operand planes are free (its predecessor's MMAs are done)
-        issue_mma(cur ^ 64u);
-        if (next + G < n_tiles) load_tile(tile_base_of(next + G), v);
-        if (next + 3 * G < n_tiles) prefetch_tile(tile_base_of(next + 3 * G));
+      if (loader) {
+        if (next < n_tiles) {
+          put_tile();  // tile `next`: the operand planes are free (the MMAs of `tile` are done)
+          asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+          asm volatile("bar.sync 1, %0;\n" ::"n"(kProdThreads) : "memory");  // loading warps only
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          issue_mma(cur ^ 64u);
+          if (next + G < n_tiles) load_tile(tile_base_of(next + G), v);
+          if (next + 3 * G < n_tiles) prefetch_tile(tile_base_of(next + 3 * G));
+        }
+      } else {
+        epilogue(tile_base_of(tile), cur);
       }
-      epilogue(tile_base_of(tile), cur);
       if (next >= n_tiles) break;
-      ok = wait_mma();  // also orders this epilogue's TMEM reads before the next MMAs into `cur`
+      // orders this epilogue's TMEM reads before the next MMAs into `cur`, and
+      // the MMAs of `next` before the next operand split
+      ok = wait_mma();
       tile = next;
       cur ^= 64u;
     }
@@ -495,7 +518,7 @@ static FusedArgs make_args(const FusedGate& g, int n) {
   a.n_out = no;
   a.lane_over_j = (F & 1ull) ? 1 : 0;
   // Sub-cube bits: 0..5 are qubits 0..5 (16-byte pairs, lanes: 512 contiguous
-  // bytes per warp), 6..8 the warp bits, 9..11 the load steps.  When column
+  // bytes per warp), 6..7 the loading warps, 8..11 the load steps.  When column
   // bit 0 (the lowest fused qubit) is not a lane qubit it becomes step bit 0
   // and lane groups run the steps rotated, so that one store covers both
   // column parities.
@@ -507,7 +530,7 @@ static FusedArgs make_args(const FusedGate& g, int n) {
     int at = -1;
     for (int b = 6; b < 12; ++b)
       if (a.sub[b] == a.q[0]) at = b;
-    std::swap(a.sub[at], a.sub[9]);
+    std::swap(a.sub[at], a.sub[8]);
     a.rot = 1;
   }
   for (int b = 0; b < 12; ++b) {
