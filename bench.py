@@ -181,19 +181,19 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def traffic_from_profile(n, amp_bytes):
-    """DRAM traffic per tiled-pass launch from the committed ncu summary
-    (bytes per amplitude per pass, scaled to this state size)."""
-    p = ROOT / "profiles" / "k_tile_pass_brickwork26_c64.md"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_amplitude_per_pass:"):
-            try:
-                return float(line.split(":")[1].split()[0]) * (1 << n)
-            except ValueError:
-                return None
-    return None
+# DRAM bytes per amplitude per launch of the dominant kernels, from ncu
+# captures (dram__bytes_read.sum + dram__bytes_write.sum of one launch divided
+# by the amplitudes it covers) on 26-qubit complex64 cases; a full-size launch
+# moves the same bytes per amplitude (every amplitude is read and written once
+# per pass), so the per-launch traffic is this figure times 2^n.
+DRAM_BYTES_PER_AMP = {
+    "k_tile_pass": 15.14,  # 26q brickwork depth 8, two launches averaged
+}
+
+
+def traffic_per_launch(kernel, n):
+    b = DRAM_BYTES_PER_AMP.get(kernel)
+    return None if b is None else b * (1 << n)
 
 
 def run_engine(args):
@@ -276,7 +276,7 @@ def run_engine(args):
     peak, peak_kind = peaks()
     avg_launch_ms = float(np.mean(launch_ms)) if launch_ms else float("nan")
     achieved = 2 * S / (avg_launch_ms / 1000.0) / 1e9
-    traffic = traffic_from_profile(n, amp_bytes)
+    traffic = traffic_per_launch("k_tile_pass", n) if args.dtype == "c64" else None
     roofline = {"bound": "hbm", "kernel": "k_tile_pass", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
@@ -309,6 +309,20 @@ def run_engine(args):
                                          "tolerance": {"one_minus_F": 1e-5, "max_abs_dZ": 1e-5}}
             extra["complex128_run"] = {"gates_per_s": G / t128, "seconds": t128,
                                        "passes": circ.plan_stats(n, "c128", args.mode)["passes"]}
+            # the same circuit through the per-gate path in complex128 (one
+            # kernel per gate, no planner): a check of the planned engine at
+            # the full size that does not rest on the planner
+            svpg = StateVector(n, "c128")
+            circ.execute(svpg, "pergate")
+            zpg = svpg.expectation_z_all()
+            extra["accuracy_vs_pergate"] = {
+                "reference": "complex128 per-gate path (one kernel per gate, no tiled plan)",
+                "tiled_c64": {"one_minus_F": 1.0 - sv.fidelity(svpg),
+                              "max_abs_dZ": float(np.abs(z_c64 - zpg).max())},
+                "tiled_c128": {"one_minus_F": 1.0 - sv128.fidelity(svpg),
+                               "max_abs_dZ": float(np.abs(z128 - zpg).max())},
+                "tolerance": {"c64": 1e-5, "c128": 1e-12}}
+            svpg.close()
             sv128.close()
         # plain per-gate path: one launch per gate, algorithmic GB/s
         pg_ms = (C.c_float * maxl)()
@@ -372,10 +386,96 @@ def run_engine(args):
             "gpu_launches": launches_per_step * args.steps, "clocks": clk,
         }
         line.update(extra)
-        print(json.dumps(line), flush=True)
     sv.close()
     circ.close()
+    if rank == 0 and world == 1 and not args.quick and not args.plain_only:
+        # the CPU-runnable configuration and the three forms, each with its own
+        # parity, e2e, CPU baseline, roofline and clock record
+        line["config1_brickwork20"] = run_config1(args)
+        sub = argparse.Namespace(**vars(args))
+        sub.qubits = 32
+        line["precision"] = run_precision(sub)
+        line["batch"] = run_batch(argparse.Namespace(**vars(args)))
+        sub = argparse.Namespace(**vars(args))
+        sub.rates = args.embedded_rates
+        line["serve"] = run_serve(sub)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     replicas.shutdown()
+
+
+def run_config1(args):
+    """The CPU-runnable configuration: 20-qubit complex128 brickwork, depth 20,
+    seeds 1-3, |0..0>; outputs the final state, all <Z_i> and 1000 shots.  The
+    engine's tiled run and the oracle's per-gate passes (the reference's CPU
+    path, restated) are both timed in full: 3 warm-up and 5 measured runs per
+    seed.  Parity: 1-F, max|amp diff| and max|d<Z_i>| against the oracle, and
+    the 1000 shots drawn with the same uniforms."""
+    import torch
+    from nqpu_b200 import _lib
+    from nqpu_b200.circuits import brickwork
+    from nqpu_b200.state import Circuit, StateVector, MODES
+    from oracle import oracle as O
+    lib = _lib.load()
+    n, depth, shots = 20, 20, 1000
+    out = {"workload": f"brickwork {n}q depth {depth} complex128, seeds 1-3, all <Z_i> + {shots} shots",
+           "per_seed": []}
+    gpu_s, cpu_s, G_tot = [], [], 0
+    for seed in (1, 2, 3):
+        gates = brickwork(n, depth, seed)
+        G = len(gates)
+        G_tot += G
+        c = Circuit(n, gates)
+        sv = StateVector(n, "c128")
+        stream = torch.cuda.ExternalStream(lib.nqpu_state_cuda_stream(sv.h_))
+        u = O.xorshift_uniforms(seed, shots)
+
+        def gpu_run():
+            sv.reset()
+            c.execute(sv, "tiled")
+            return sv.expectation_z_all(), sv.sample_with_uniforms(u)
+        for _ in range(3):
+            gpu_run()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(5):
+            z, smp = gpu_run()
+        ev1.record(stream)
+        ev1.synchronize()
+        g_ms = ev0.elapsed_time(ev1) / 5
+        amps = sv.amplitudes()
+
+        def cpu_run():
+            o = O.OracleState(n)
+            o.apply(gates)
+            return o, o.expectation_z_all(), o.sample_uniforms(u)
+        for _ in range(3):
+            cpu_run()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            o, zo, so = cpu_run()
+        c_ms = 1000 * (time.perf_counter() - t0) / 5
+        ref = o.amplitudes()
+        f = abs(np.vdot(ref, amps)) ** 2
+        out["per_seed"].append({
+            "seed": seed, "gates": G, "gpu_ms": g_ms, "cpu_ms": c_ms,
+            "one_minus_F": 1 - f, "max_abs_amp_diff": float(np.abs(amps - ref).max()),
+            "max_abs_dZ": float(np.abs(z - zo).max()),
+            "shots_equal": int(np.sum(np.asarray(smp) == np.asarray(so))), "shots": shots})
+        gpu_s.append(g_ms / 1000)
+        cpu_s.append(c_ms / 1000)
+        sv.close()
+        c.close()
+    out["gpu_gates_per_s"] = G_tot / sum(gpu_s)
+    out["cpu_baseline"] = {"value": G_tot / sum(cpu_s), "unit": "gates/s", "cores": O.max_threads(),
+                           "kind": "port", "sample": "the full circuit of each seed, 3 warm-up + 5 timed runs, "
+                                                     "per-gate passes + all <Z_i> + 1000 shots"}
+    out["speedup_vs_cpu"] = out["gpu_gates_per_s"] / out["cpu_baseline"]["value"]
+    out["tolerance"] = {"one_minus_F": 1e-12, "max_abs_amp_diff": 1e-12, "max_abs_dZ": 1e-12,
+                        "shots": "equal up to CDF summation ties"}
+    out["timing"] = "gpu: CUDA events on the state's stream around 5 runs (reset, tiled circuit, all <Z_i>, " \
+                    "1000 shots with host read-back); cpu: wall clock around 5 oracle runs"
+    return out
 
 
 def run_precision(args):
@@ -487,7 +587,7 @@ def run_precision(args):
         "fp64_reference_seconds": sum(l128) / 1000, "plain_tiled_c64": plain,
         "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": len(l64), "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_batch(args):
@@ -650,8 +750,8 @@ def run_batch(args):
         "host_build_s": host_build_s, "prepare_s": prepare_s, "wall_s_timed": wall,
         "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": steps, "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
     b.close()
+    return line
 
 
 def run_serve(args):
@@ -802,9 +902,9 @@ def run_serve(args):
                           "uniforms go host->device, its <Z_i> or outcomes device->host, inside the span"},
         "cpu_baseline": cpu, "gpu_launches": launches * len(rates), "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
     for c in circs:
         c.close()
+    return line
 
 
 def main():
@@ -840,6 +940,10 @@ def main():
                     help="serve form: offered rates (requests/s); the last one saturates the server")
     ap.add_argument("--lanes", type=int, default=16, help="serve form: concurrent requests on the device")
     ap.add_argument("--serve-budget-gb", type=float, default=64.0, help="serve form: HBM budget for states")
+    ap.add_argument("--embedded-rates", default="40,160,640",
+                    help="serve rates of the serve block inside the default (plain) line")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="default run: only the plain 30q line (no config-1, precision, batch, serve blocks)")
     ap.add_argument("--verbose", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and not args.quick:
@@ -847,13 +951,13 @@ def main():
     if args.impl == "reference":
         run_reference(args)
     elif args.form == "batch":
-        run_batch(args)
+        print(json.dumps(run_batch(args)), flush=True)
     elif args.form == "serve":
-        run_serve(args)
+        print(json.dumps(run_serve(args)), flush=True)
     elif args.form == "precision":
         if args.qubits == 30:
             args.qubits = 32
-        run_precision(args)
+        print(json.dumps(run_precision(args)), flush=True)
     else:
         run_engine(args)
 

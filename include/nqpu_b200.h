@@ -236,18 +236,20 @@ NqpuError    nqpu_circuit_add_custom_1q(NqpuCircuit* c, uint32_t q, const NqpuCo
 NqpuError    nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uint32_t q2, const NqpuComplex* matrix);
 /* No counterpart in the reference.  All <Z_i> (FP64) of a state that lives in
  * the CALLER's device memory, for callers that cannot allocate device memory:
- * code running while a stream is captured into a CUDA graph, plugins whose
- * host runtime owns the device memory pool, real-time loops that must not wait
- * on the allocator.  It allocates nothing: the reduction's scratch is a fixed
- * array in this library's device module (about 2.2 MB on every GPU that loads
- * the library, kept until exit).  d_amplitudes: 2^n interleaved (re, im)
- * amplitudes of `dtype`, 16-byte aligned; d_out: n doubles in device memory;
- * cuda_stream: a cudaStream_t (NULL = legacy default stream).  The work is only
- * queued; synchronise the stream before reading d_out.  Limit: complex64 states
- * up to 28 qubits, complex128 up to 27; larger states return
- * NQPU_INVALID_PARAMETER.  The first call on a device resolves the scratch
- * address and should come before any stream capture.  Calls share the scratch,
- * so calls whose kernels overlap on the GPU race. */
+ * plugins whose host runtime owns the device memory pool, real-time loops that
+ * must not wait on the allocator, code running while its stream is captured
+ * (where cudaMalloc is not permitted).  It allocates nothing: the reduction's
+ * scratch is a fixed array in this library's device module (about 2.2 MB on
+ * every GPU that loads the library, kept until exit).  d_amplitudes: 2^n
+ * interleaved (re, im) amplitudes of `dtype`, 16-byte aligned; d_out: n doubles
+ * in device memory; cuda_stream: a cudaStream_t (NULL = legacy default
+ * stream).  The work is only queued; synchronise the stream before reading
+ * d_out.  Limit: complex64 states up to 28 qubits, complex128 up to 27; larger
+ * states return NQPU_INVALID_PARAMETER.  The first call on a device (with that
+ * device current) resolves the scratch address in the device's primary
+ * context and should come before any stream capture; the address is not valid
+ * after cudaDeviceReset.  Calls share the scratch, so calls whose kernels
+ * overlap on the GPU race. */
 NqpuError   nqpu_expectation_z_all_noalloc(const void* d_amplitudes, uint32_t num_qubits,
                                            NqpuDtype dtype, double* d_out, void* cuda_stream);
 
@@ -333,7 +335,15 @@ typedef enum {
     NQPU_BATCH_SMALL_MAX_QUBITS = 0, /* circuits up to this size run in one CTA's shared memory (5..13) */
     NQPU_BATCH_TILE_QUBITS      = 1, /* tile bits of the larger circuits' passes (10..13) */
     NQPU_BATCH_QUEUE_ORDER      = 2, /* 0: small circuits between pass rounds, 1: first, 2: last */
-    NQPU_BATCH_CTAS_PER_SM      = 3  /* persistent CTAs per SM (1..2) */
+    NQPU_BATCH_CTAS_PER_SM      = 3, /* persistent CTAs per SM (1..2) */
+    /* Polls of a pass tile's bounded dependency wait (>= 1; default 2^26, each
+     * poll ~64 ns or more).  When a wait expires, every CTA stops, and
+     * nqpu_batch_run returns NQPU_SIMULATION_FAILED; the handle stays usable. */
+    NQPU_BATCH_SPIN_LIMIT       = 4,
+    /* Failure injection for tests of the bounded waits (0 or 1): 1 leaves the
+     * first tile of the first large circuit's first pass out of the queue, so
+     * the waits of that circuit's next pass cannot succeed and expire. */
+    NQPU_BATCH_DROP_TILE        = 5
 } NqpuBatchParam;
 
 NqpuBatch*  nqpu_batch_create(void);
@@ -395,8 +405,15 @@ NqpuError   nqpu_server_wait(NqpuServer* server, uint64_t request_id, double tim
  * running, total milliseconds from submit to completion. */
 NqpuError   nqpu_server_result(NqpuServer* server, uint64_t request_id, double* out_z, uint32_t z_len,
                                uint64_t* out_shots, uint32_t shots_len, double* timing_ms);
+/* Withdraw a request that is still queued (not yet admitted to a lane): it
+ * never runs and its id is forgotten (later calls with it return
+ * NQPU_INVALID_HANDLE).  NQPU_INVALID_PARAMETER when the request is already
+ * running or finished (it completes normally); NQPU_INVALID_HANDLE for an
+ * unknown id. */
+NqpuError   nqpu_server_cancel(NqpuServer* server, uint64_t request_id);
 /* out[0..7] = submitted, completed, failed, running, queued, peak resident
- * bytes, arena bytes, peak concurrent requests.  len >= 8. */
+ * bytes, arena bytes, peak concurrent requests; out[8] (len >= 9) = cancelled
+ * requests.  len >= 8. */
 NqpuError   nqpu_server_stats(NqpuServer* server, uint64_t* out, uint32_t len);
 
 #ifdef __cplusplus

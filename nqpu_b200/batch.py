@@ -11,7 +11,8 @@ from . import _lib
 from ._lib import check
 from .state import Circuit
 
-PARAMS = {"small_max_qubits": 0, "tile_qubits": 1, "queue_order": 2, "ctas_per_sm": 3}
+PARAMS = {"small_max_qubits": 0, "tile_qubits": 1, "queue_order": 2, "ctas_per_sm": 3, "spin_limit": 4,
+          "drop_tile": 5}
 
 
 class Batch:

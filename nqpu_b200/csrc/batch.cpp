@@ -29,6 +29,8 @@ struct BatchImpl {
   int plan_kmax = 13;    // tile bits of the larger circuits' passes
   int order = 0;         // queue order strategy
   int ctas_per_sm = 2;
+  uint32_t spin_limit = kBatchSpinLimit;  // polls of a bounded dependency wait
+  bool drop_tile = false;                 // failure injection: leave one pass-0 tile out of the queue
   bool built = false;
   cudaStream_t stream = nullptr;
   float* d_arena = nullptr;
@@ -171,12 +173,23 @@ static cudaError_t batch_build(BatchImpl* b) {
     for (; si < std::min(upto, small.size()); ++si) tasks.push_back(BatchTask{small[si], -1, 0, 0});
   };
   if (b->order == 1) push_small(small.size());
+  bool dropped = false;
   for (int r = 0; r < max_rounds; ++r) {
     for (int ci : large) {
       const BatchCirc& C = circs[ci];
       if (r > C.n_passes) continue;
       const uint32_t tiles = r < C.n_passes ? (1u << passes[C.pass_base + r].n_out) : uint32_t(C.meas_tiles);
-      for (uint32_t t = 0; t < tiles; ++t) tasks.push_back(BatchTask{ci, r, t, 0});
+      for (uint32_t t = 0; t < tiles; ++t) {
+        // failure injection (tests): the first tile of the first large
+        // circuit's first pass is never queued, so that circuit's pass-1
+        // tiles wait on a counter that cannot complete and their bounded
+        // waits expire
+        if (b->drop_tile && !dropped && r == 0) {
+          dropped = true;
+          continue;
+        }
+        tasks.push_back(BatchTask{ci, r, t, 0});
+      }
     }
     if (b->order == 0) push_small(small.size() * size_t(r + 1) / size_t(max_rounds));
   }
@@ -211,6 +224,7 @@ static cudaError_t batch_build(BatchImpl* b) {
   L.counters = b->d_counters; L.partials = b->d_partials; L.results = b->d_results;
   L.cursor = b->d_cursor; L.err = b->d_err;
   L.grid = unsigned(std::max(1, device_sms() * b->ctas_per_sm));
+  L.spin_limit = b->spin_limit;
   // warm the module and the smem attribute outside the capture
   if ((e = cudaMemsetAsync(b->d_cursor, 0xFF, sizeof(uint32_t), b->stream)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream)) != cudaSuccess) return e;
@@ -295,6 +309,14 @@ extern "C" NqpuError nqpu_batch_config(NqpuBatch* batch, NqpuBatchParam param, i
     case NQPU_BATCH_CTAS_PER_SM:
       if (value < 1 || value > 2) return NQPU_INVALID_PARAMETER;
       b->ctas_per_sm = value;
+      break;
+    case NQPU_BATCH_SPIN_LIMIT:
+      if (value < 1) return NQPU_INVALID_PARAMETER;
+      b->spin_limit = uint32_t(value);
+      break;
+    case NQPU_BATCH_DROP_TILE:
+      if (value < 0 || value > 1) return NQPU_INVALID_PARAMETER;
+      b->drop_tile = value == 1;
       break;
     default:
       return NQPU_INVALID_PARAMETER;

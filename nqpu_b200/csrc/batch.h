@@ -43,7 +43,11 @@ struct BatchLaunch {
   uint32_t* cursor;
   int* err;
   unsigned grid;
+  uint32_t spin_limit;  // polls of a bounded dependency wait (0: kBatchSpinLimit)
 };
+
+// Default bound of a pass tile's dependency wait (polls of ~64 ns or more).
+constexpr uint32_t kBatchSpinLimit = 1u << 26;
 
 size_t batch_smem_bytes();
 cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s);

@@ -602,7 +602,8 @@ extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t
   } catch (...) {
     return NQPU_ALLOCATION_FAILED;
   }
-  for (uint32_t i = 0; i < count; ++i) {
+  // index arithmetic in size_t: 16 * count overflows 32 bits above 2^28 gates
+  for (size_t i = 0; i < size_t(count); ++i) {
     if (codes[i] >= uint32_t(G_COUNT)) return NQPU_INVALID_PARAMETER;
     GateRec g = mk(uint8_t(codes[i]), qubits[3 * i], qubits[3 * i + 1], qubits[3 * i + 2], params[4 * i],
                    params[4 * i + 1], params[4 * i + 2], params[4 * i + 3]);

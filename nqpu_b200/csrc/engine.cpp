@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include "device_once.h"
 #include "fused.h"
 #include "kernels.h"
 
@@ -13,7 +14,6 @@ namespace nqpu {
 namespace {
 std::once_flag g_dev_once;
 bool g_dev_ok = false;
-int g_sms = 148;
 
 void dev_init() {
   int count = 0;
@@ -22,14 +22,6 @@ void dev_init() {
     g_dev_ok = false;
     return;
   }
-  int dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceProp p;
-  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
-    g_dev_ok = false;
-    return;
-  }
-  g_sms = p.multiProcessorCount;
   g_dev_ok = true;
 }
 }  // namespace
@@ -39,9 +31,16 @@ bool device_ready() {
   return g_dev_ok;
 }
 
+// SM count of the current device (grids are sized in multiples of it), read
+// once per device.
 int device_sms() {
-  device_ready();
-  return g_sms;
+  static PerDeviceOnce<int> sms;
+  int dev = 0;
+  if (!device_ready() || cudaGetDevice(&dev) != cudaSuccess) return 148;
+  return sms.get(dev, [dev] {
+    int v = 0;
+    return (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) ? v : 148;
+  }, 148);
 }
 
 StateImpl* state_new(uint32_t n, DType dt) {

@@ -15,7 +15,8 @@ namespace nqpu {
 
 double next_random_f64();
 
-// Device context (one GPU; the engine uses the current device at first use).
+// Device context: device_ready() is true when a CUDA device exists; work runs
+// on the caller's current device, and device_sms() is that device's SM count.
 bool device_ready();
 int device_sms();
 

@@ -37,6 +37,7 @@
 #include <cstring>
 #include <vector>
 
+#include "device_once.h"
 #include "engine.h"
 #include "fused.h"
 #include "fusion.h"
@@ -321,7 +322,10 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
                    : "memory");
     }
   };
-  // bounded wait for the last MMAs issued; false: the CTA gives up (error flagged)
+  // bounded wait for the last MMAs issued; false: the CTA gives up (error
+  // flagged).  No MMA is issued after a wait that expired, and the MMAs it was
+  // waiting for get one more bounded wait before the CTA leaves its tile loop
+  // for the normal exit, which frees their TMEM accumulators.
   auto wait_mma = [&]() {
     uint32_t it = 0;
     bool done = false;
@@ -330,6 +334,8 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedCtasPerSm)
     if (!done) {
       atomicExch(err, 1);
       abort_flag = 1;
+      for (uint32_t j = 0; j < 4 * kWaitLimit && !mbar_try_wait(mbar_addr, phase); ++j) {
+      }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -601,12 +607,14 @@ void fused_plan_free(void* plan) {
 cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
   auto* p = static_cast<FusedPlanImpl*>(plan);
   if (!p || s->dt != DType::C64 || int(s->n) != p->n) return cudaErrorInvalidValue;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_fused_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFused);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  // the shared-memory limit is a per-device attribute: set once per device
+  static PerDeviceOnce<cudaError_t> attr;
+  int dev = 0;
+  cudaError_t ae = cudaGetDevice(&dev);
+  if (ae != cudaSuccess) return ae;
+  ae = attr.get(dev, [] { return cudaFuncSetAttribute(k_fused_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFused); },
+                cudaErrorInvalidDevice);
+  if (ae != cudaSuccess) return ae;
   const int n = p->n;
   const uint64_t n_tiles = 1ull << (n - 12);
   const unsigned grid = unsigned(std::min<uint64_t>(n_tiles, uint64_t(p->norm_slots)));

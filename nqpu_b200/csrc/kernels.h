@@ -46,7 +46,19 @@ cudaError_t launch_convert(DType src_dt, const void* src, DType dst_dt, void* ds
                            cudaStream_t s, int num_sms);
 
 // --- FP64 reductions ---------------------------------------------------------
-// Scratch layout requirements are returned by reduce_scratch_bytes(n).
+// Layout of the all-<Z_i> scratch (doubles): kZsMaxBlocks x kZsBlkVals
+// per-block low-bit partials, then one total per segment of kZsSegVecs 128-bit
+// vectors (room is kept for kZsSegSlots per segment).
+constexpr int kZsBlkVals = 16;
+constexpr int kZsMaxBlocks = 1024;
+constexpr uint64_t kZsSegVecs = 256 * 16;  // threads per block x vectors per thread
+constexpr int kZsSegSlots = 8;
+// Doubles of all-<Z_i> scratch for a state of 2^vec_log2 128-bit vectors.
+constexpr size_t zsums_scratch_doubles(int vec_log2) {
+  return size_t(kZsMaxBlocks) * kZsBlkVals +
+         size_t(((uint64_t(1) << vec_log2) + kZsSegVecs - 1) / kZsSegVecs) * kZsSegSlots;
+}
+// Scratch bytes every reduction below needs on an n-qubit state.
 size_t reduce_scratch_bytes(int n);
 // out[0] = sum |a|^2, out[1+q] = sum over amplitudes with bit q set of |a|^2, q < n.
 cudaError_t launch_zsums(DType dt, const void* amp, int n, double* scratch, double* out,

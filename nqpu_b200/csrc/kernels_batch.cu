@@ -25,6 +25,7 @@
 // uses byte lookup tables of bond sums, sum_i J_i z_i z_{i+1} = Jtot - 2 sum of
 // J_i over the set bits of x ^ (x >> 1).
 #include "batch.h"
+#include "device_once.h"
 #include "kernels.h"
 #include "tile_device.cuh"
 
@@ -32,7 +33,6 @@ namespace nqpu {
 
 constexpr int kBatchK = 13;                       // complex64 tile bits
 constexpr uint32_t kBatchVec = 1u << (kBatchK - 1);
-constexpr uint32_t kSpinLimit = 1u << 26;         // bounded dependency wait
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
   uint32_t v;
@@ -40,14 +40,16 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
   return v;
 }
 
-// CTA-wide wait until *ctr >= target; returns false on timeout.
-__device__ __forceinline__ bool wait_counter(const uint32_t* ctr, uint32_t target, int* err, int* s_flag) {
+// CTA-wide wait until *ctr >= target, at most `limit` polls; returns false on
+// timeout (and flags the error for every CTA).
+__device__ __forceinline__ bool wait_counter(const uint32_t* ctr, uint32_t target, uint32_t limit, int* err,
+                                             int* s_flag) {
   if (threadIdx.x == 0) {
     uint32_t it = 0;
     bool ok = true;
     while (ld_acquire(ctr) < target) {
       // give up on an expired limit, or at once when another CTA already failed
-      if (++it >= kSpinLimit || ld_acquire(reinterpret_cast<const uint32_t*>(err)) != 0) {
+      if (++it >= limit || ld_acquire(reinterpret_cast<const uint32_t*>(err)) != 0) {
         ok = false;
         atomicExch(err, 2);
         break;
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             uint32_t n_tasks, const PassRec* __restrict__ passes, const StageRec* __restrict__ stages,
             const TileOp<float>* __restrict__ ops, const double* __restrict__ obs, uint32_t* __restrict__ counters,
             double* __restrict__ partials, double* __restrict__ results, uint32_t* __restrict__ cursor,
-            int* __restrict__ err) {
+            int* __restrict__ err, uint32_t spin_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* sv = reinterpret_cast<float4*>(smem_raw);
   uint64_t* hi_off = reinterpret_cast<uint64_t*>(smem_raw + sizeof(float4) * kBatchVec);
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       load_pass(C, T.phase);
       if (T.phase > 0) {
         const uint32_t need = 1u << passes[C.pass_base + T.phase - 1].n_out;
-        if (!wait_counter(counters + C.done_base + T.phase - 1, need, err, &s_flag)) continue;
+        if (!wait_counter(counters + C.done_base + T.phase - 1, need, spin_limit, err, &s_flag)) continue;
       }
       const int k = P.k, c = P.c;
       const uint32_t nvec = 1u << (k - 1);
@@ -248,7 +250,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     // ---- one measurement tile ----
     {
       const uint32_t need = 1u << passes[C.pass_base + C.n_passes - 1].n_out;
-      if (!wait_counter(counters + C.done_base + C.n_passes - 1, need, err, &s_flag)) continue;
+      if (!wait_counter(counters + C.done_base + C.n_passes - 1, need, spin_limit, err, &s_flag)) continue;
     }
     double jtot;
     load_obs(C, &jtot);
@@ -281,15 +283,18 @@ size_t batch_smem_bytes() {
 }
 
 cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s) {
-  static bool configured = false;
   const size_t smem = batch_smem_bytes();
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  // the shared-memory limit is a per-device attribute: set once per device
+  static PerDeviceOnce<cudaError_t> attr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = attr.get(dev, [&] { return cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); },
+               cudaErrorInvalidDevice);
+  if (e != cudaSuccess) return e;
   k_batch<<<L.grid, kTileThreads, smem, s>>>(L.arena, L.circs, L.tasks, L.n_tasks, L.passes, L.stages, L.ops,
-                                            L.obs, L.counters, L.partials, L.results, L.cursor, L.err);
+                                            L.obs, L.counters, L.partials, L.results, L.cursor, L.err,
+                                            L.spin_limit ? L.spin_limit : kBatchSpinLimit);
   return cudaGetLastError();
 }
 

@@ -44,11 +44,11 @@ __device__ __forceinline__ void vec_probs<double>(const double2& v, double* p) {
   p[0] = v.x * v.x + v.y * v.y;
 }
 
-// Layout of the zsums scratch (doubles):
+// Layout of the zsums scratch (doubles, kernels.h):
 //   [0, nblk*kBlkVals)            per-block low-bit partials
-//   [kZsMaxBlocks*kBlkVals, + nseg) per-segment totals (room is kept for 8 per segment)
-constexpr int kBlkVals = 16;  // tot, bit0(c64), 8 thread bits, 4 j bits, (pad)
-constexpr int kZsMaxBlocks = 1024;
+//   [kZsMaxBlocks*kBlkVals, + nseg) per-segment totals
+constexpr int kBlkVals = kZsBlkVals;  // tot, bit0(c64), 8 thread bits, 4 j bits, (pad)
+static_assert(kZsSegVecs == uint64_t(kRedThreads) * kRedVecPerThread, "segment size");
 
 template <typename Real>
 __global__ void __launch_bounds__(kRedThreads)
@@ -178,13 +178,11 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
-static uint64_t seg_vecs() { return uint64_t(kRedThreads) * kRedVecPerThread; }
+static uint64_t seg_vecs() { return kZsSegVecs; }
 
 size_t reduce_scratch_bytes(int n) {
   // worst case complex128: one vector per amplitude
-  const uint64_t nvec = 1ull << n;
-  const uint64_t nseg = (nvec + seg_vecs() - 1) / seg_vecs();
-  size_t zs = sizeof(double) * (size_t(kZsMaxBlocks) * kBlkVals + nseg * 8);
+  size_t zs = sizeof(double) * zsums_scratch_doubles(n);
   size_t samp = sizeof(double) * (2 * ((1ull << n) / 4096 + 2) + 64);
   size_t inner = sizeof(double) * (2 * 4096 + 64);
   return std::max(zs, std::max(samp, inner)) + 4096;

@@ -17,6 +17,7 @@
 // Shared-memory layout: vector u (16 B) lives at slot swz(u) = u ^ fold3(u>>3)
 // so that the 8 lanes of a quarter-warp that the planner maps to vector bits of
 // distinct residue mod 3 hit 8 distinct 16-byte bank groups.
+#include "device_once.h"
 #include "kernels.h"
 #include "tile_device.cuh"
 
@@ -163,12 +164,14 @@ cudaError_t launch_tile_pass_cfg(Real* amp, const PassRec& host_pass, const Pass
   const size_t smem_max = tile_smem_bytes<Real, KMAX>(MINB);
   const size_t smem = smem_max - sizeof(uint32_t) * kStageTabWords *
                                      size_t(kMaxPassStages - (host_pass.stage_end - host_pass.stage_begin));
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  // the shared-memory limit is a per-device attribute: set once per device
+  static PerDeviceOnce<cudaError_t> attr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = attr.get(dev, [&] { return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)); },
+               cudaErrorInvalidDevice);
+  if (e != cudaSuccess) return e;
   const uint64_t n_tiles = 1ull << host_pass.n_out;
   const uint64_t max_ctas = uint64_t(num_sms) * MINB;
   const unsigned grid = unsigned(n_tiles < max_ctas ? n_tiles : max_ctas);

@@ -174,7 +174,7 @@ struct ServerImpl {
   std::thread worker;
   bool stop = false;
   uint64_t next_id = 1;
-  uint64_t submitted = 0, completed = 0, failed = 0, running = 0, large_running = 0;
+  uint64_t submitted = 0, completed = 0, failed = 0, running = 0, large_running = 0, cancelled = 0;
   uint64_t peak_used = 0, peak_running = 0;
 };
 
@@ -536,6 +536,23 @@ extern "C" NqpuError nqpu_server_result(NqpuServer* server, uint64_t request_id,
   return NQPU_OK;
 }
 
+extern "C" NqpuError nqpu_server_cancel(NqpuServer* server, uint64_t request_id) {
+  if (!server) return NQPU_NULL_POINTER;
+  ServerImpl* sv = SV(server);
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(request_id);
+  if (it == sv->reqs.end()) return NQPU_INVALID_HANDLE;
+  // status is set to running under this lock when the worker admits a request,
+  // so a request still queued here is still in `pending`
+  if (it->second->status != 0) return NQPU_INVALID_PARAMETER;  // admitted: it runs to completion
+  auto pit = std::find(sv->pending.begin(), sv->pending.end(), it->second);
+  if (pit != sv->pending.end()) sv->pending.erase(pit);
+  sv->reqs.erase(it);
+  sv->cancelled++;
+  sv->cv_done.notify_all();  // wait(0) may now be satisfied
+  return NQPU_OK;
+}
+
 extern "C" NqpuError nqpu_server_stats(NqpuServer* server, uint64_t* out, uint32_t len) {
   if (!server || !out) return NQPU_NULL_POINTER;
   if (len < 8) return NQPU_INVALID_PARAMETER;
@@ -549,5 +566,6 @@ extern "C" NqpuError nqpu_server_stats(NqpuServer* server, uint64_t* out, uint32
   out[5] = sv->peak_used;
   out[6] = sv->arena_bytes;
   out[7] = sv->peak_running;
+  if (len >= 9) out[8] = sv->cancelled;
   return NQPU_OK;
 }

@@ -60,6 +60,16 @@ class Server:
     def wait(self, rid: int = 0, timeout_s: float = 0.0):
         check(self.lib.nqpu_server_wait(self.h_, rid, float(timeout_s)), "server_wait")
 
+    def cancel(self, rid: int) -> bool:
+        """Withdraw a queued request: True when it was still queued (it never
+        runs and its id is forgotten), False when it was already admitted."""
+        err = self.lib.nqpu_server_cancel(self.h_, rid)
+        if err == 2:  # NQPU_INVALID_PARAMETER: already running or finished
+            return False
+        check(err, "server_cancel")
+        self.meta.pop(rid, None)
+        return True
+
     def result(self, rid: int):
         """(values, timing) for a finished request: values = <Z_i> array (zall) or
         outcome array (shots); timing = {queued_ms, running_ms, total_ms}."""
@@ -78,8 +88,8 @@ class Server:
         return vals, {"queued_ms": t[0], "running_ms": t[1], "total_ms": t[2]}
 
     def stats(self) -> dict:
-        out = (C.c_uint64 * 8)()
-        check(self.lib.nqpu_server_stats(self.h_, out, 8), "server_stats")
+        out = (C.c_uint64 * 9)()
+        check(self.lib.nqpu_server_stats(self.h_, out, 9), "server_stats")
         keys = ("submitted", "completed", "failed", "running", "queued", "peak_resident_bytes", "arena_bytes",
-                "peak_concurrent")
+                "peak_concurrent", "cancelled")
         return {k: int(v) for k, v in zip(keys, out)}

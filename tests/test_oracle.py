@@ -25,6 +25,36 @@ def test_oracle_matches_reference_python_golden(case):
     np.testing.assert_allclose(o.amplitudes(), ref, atol=1e-13, rtol=0)
 
 
+def align_global_phase(got, ref):
+    """got times the one global phase that best matches ref."""
+    ov = np.vdot(got, ref)
+    return got * (ov / abs(ov))
+
+
+@pytest.mark.parametrize("case", range(22))
+def test_oracle_u3_rzz_match_reference_python_golden(case):
+    # U3 (ascii_viz.rs:134-150) and RZZ (gates.rs:486) against the reference's
+    # Python statevector running Rz Ry Rz and CX Rz CX: RZZ circuits agree
+    # exactly, U3 ones up to one global phase (e^{i(phi+lambda)/2} per U3)
+    n, gates, ref = make_golden.load_u3_rzz()[case]
+    o = OracleState(n)
+    o.apply(gates)
+    got = o.amplitudes()
+    if any(g[0] == "u3" for g in gates):
+        got = align_global_phase(got, ref)
+    np.testing.assert_allclose(got, ref, atol=1e-12, rtol=0)
+
+
+def test_oracle_rzz_alone_matches_exactly():
+    # no global-phase freedom: RZZ = CX Rz CX exactly
+    cases = [c for c in make_golden.load_u3_rzz() if not any(g[0] == "u3" for g in c[1])]
+    assert len(cases) == 4 and all(any(g[0] == "rzz" for g in c[1]) for c in cases)
+    for n, gates, ref in cases:
+        o = OracleState(n)
+        o.apply(gates)
+        np.testing.assert_allclose(o.amplitudes(), ref, atol=1e-12, rtol=0)
+
+
 @pytest.mark.parametrize("case", [3, 9, 15])
 def test_oracle_f32_matches_golden_within_f32(case):
     n, gates, ref = make_golden.load()[case]
