@@ -276,8 +276,10 @@ def run_engine(args):
     peak, peak_kind = peaks()
     avg_launch_ms = float(np.mean(launch_ms)) if launch_ms else float("nan")
     achieved = 2 * S / (avg_launch_ms / 1000.0) / 1e9
-    traffic = traffic_per_launch("k_tile_pass", n) if args.dtype == "c64" else None
-    roofline = {"bound": "hbm", "kernel": "k_tile_pass", "achieved": achieved, "peak": peak,
+    kernel = {"tiled": "k_tile_pass", "tensor": "k_tc_pass", "fused": "k_fused_apply",
+              "pergate": "k_pg_*"}[args.mode]
+    traffic = traffic_per_launch(kernel, n) if args.dtype == "c64" else None
+    roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
                 "launches_per_step": stats["passes"], "avg_launch_ms": avg_launch_ms,
@@ -918,7 +920,7 @@ def main():
     ap.add_argument("--circuit", default="brickwork", choices=["brickwork", "qft"],
                     help="plain form circuit: random brickwork (headline) or the QFT")
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
-    ap.add_argument("--mode", default="tiled", choices=["tiled", "pergate", "fused"])
+    ap.add_argument("--mode", default="tiled", choices=["tiled", "pergate", "fused", "tensor"])
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--tile-ctas", type=int, default=0, help="tiled kernel CTAs per SM (1 or 2; 0 = library default)")
     ap.add_argument("--e2e-steps", type=int, default=2)

@@ -147,7 +147,9 @@ typedef enum { NQPU_C128 = 0, NQPU_C64 = 1 } NqpuDtype;
 typedef enum {
     NQPU_MODE_TILED   = 0,  /* multi-gate smem/register tiled passes (default)       */
     NQPU_MODE_PERGATE = 1,  /* one full-state kernel launch per gate (plain per-gate) */
-    NQPU_MODE_FUSED   = 2   /* <=5-qubit fusion, split-TF32 tcgen05 contractions      */
+    NQPU_MODE_FUSED   = 2,  /* <=5-qubit fusion, split-TF32 tcgen05 contractions      */
+    NQPU_MODE_TENSOR  = 3   /* complex64, n >= 12: up to 2 fused 5-qubit unitaries per
+                               HBM pass, split-TF32 tcgen05 GEMMs on a shared-memory tile */
 } NqpuMode;
 
 /* Like nqpu_state_create with a dtype; 1 <= n <= 34 (HBM-bounded). */

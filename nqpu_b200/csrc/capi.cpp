@@ -629,10 +629,11 @@ extern "C" NqpuError nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuSta
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;  // c_ffi.rs:1360
-  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED)
+  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED && mode != NQPU_MODE_TENSOR)
     return NQPU_INVALID_PARAMETER;
-  // the fused mode runs complex64 states of >= 12 qubits (5 fused + 7 group bits)
-  if (mode == NQPU_MODE_FUSED && (s->dt != DType::C64 || s->n < 12)) return NQPU_INVALID_PARAMETER;
+  // the fused and tensor modes run complex64 states of >= 12 qubits (5 fused + 7 row bits)
+  if ((mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) && (s->dt != DType::C64 || s->n < 12))
+    return NQPU_INVALID_PARAMETER;
   cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode));
   if (e != cudaSuccess) return map_cuda(e);
   NQ_TRY(cudaStreamSynchronize(s->stream));
@@ -645,9 +646,10 @@ extern "C" NqpuError nqpu_circuit_execute_measured(const NqpuCircuit* circuit, N
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;
-  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED)
+  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED && mode != NQPU_MODE_TENSOR)
     return NQPU_INVALID_PARAMETER;
-  if (mode == NQPU_MODE_FUSED && (s->dt != DType::C64 || s->n < 12)) return NQPU_INVALID_PARAMETER;
+  if ((mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) && (s->dt != DType::C64 || s->n < 12))
+    return NQPU_INVALID_PARAMETER;
   uint32_t nmeas = 0;
   for (const GateRec& g : c->gates) nmeas += g.code == G_MEASURE ? 1u : 0u;
   if (nmeas > 0 && (!outcomes || len < nmeas)) return NQPU_INVALID_PARAMETER;
@@ -666,7 +668,8 @@ extern "C" NqpuError nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState*
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;
-  if (mode == NQPU_MODE_FUSED && (s->dt != DType::C64 || s->n < 12)) return NQPU_INVALID_PARAMETER;
+  if ((mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) && (s->dt != DType::C64 || s->n < 12))
+    return NQPU_INVALID_PARAMETER;
   std::vector<cudaEvent_t> ev;
   cudaError_t e = circuit_run(const_cast<CircuitImpl*>(c), s, int(mode), &ev);
   cudaError_t e2 = cudaStreamSynchronize(s->stream);

@@ -8,6 +8,7 @@
 #include "device_once.h"
 #include "fused.h"
 #include "kernels.h"
+#include "tcrun.h"
 
 namespace nqpu {
 
@@ -234,6 +235,7 @@ static void plan_free(DevicePlan* p) {
   if (p->d_stages) cudaFree(p->d_stages);
   if (p->d_ops) cudaFree(p->d_ops);
   if (p->fused) fused_plan_free(p->fused);
+  if (p->tc) tc_plan_free(p->tc);
   delete p;
 }
 
@@ -273,6 +275,8 @@ static bool plan_host(const CircuitImpl* c, const Segment& seg, uint32_t n, DTyp
   } else if (mode == NQPU_MODE_FUSED) {
     p->stats.ops = p->ops.size();
     return fused_plan_build(p->ops, int(n), dt, &p->fused, &p->stats);
+  } else if (mode == NQPU_MODE_TENSOR) {
+    return tc_plan_build(p->ops, int(n), dt, &p->tc, &p->stats);
   } else {
     p->stats.passes = p->ops.size();
     p->stats.ops = p->ops.size();
@@ -285,9 +289,11 @@ bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, Pl
   for (const Segment& seg : circuit_segments(c->gates)) {
     DevicePlan p;
     PlanStats st;
-    if (mode == NQPU_MODE_FUSED) {
+    if (mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) {
       p.ops = lower_circuit(std::vector<GateRec>(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end)));
-      if (!fused_plan_stats(p.ops, int(n), dt, &st)) return false;
+      const bool ok = mode == NQPU_MODE_FUSED ? fused_plan_stats(p.ops, int(n), dt, &st)
+                                              : tc_plan_stats(p.ops, int(n), dt, &st);
+      if (!ok) return false;
     } else {
       if (!plan_host(c, seg, n, dt, mode, &p)) return false;
       st = p.stats;
@@ -412,6 +418,11 @@ static cudaError_t segment_run(CircuitImpl* c, const Segment& seg, int si, State
     e = fused_run(p->fused, s, events);
     if (e != cudaSuccess) return e;
     return fused_check_error(p->fused, s->stream);  // bounded-wait expiry flag
+  }
+  if (effective == NQPU_MODE_TENSOR) {
+    e = tc_run(p->tc, s, events);
+    if (e != cudaSuccess) return e;
+    return tc_check_error(p->tc, s->stream);  // bounded-wait expiry flag
   }
   for (size_t i = 0; i < p->tile.passes.size(); ++i) {
     e = launch_tile_pass(s->dt, s->amp, int(s->n), p->tile.passes[i], p->d_passes, p->d_stages,

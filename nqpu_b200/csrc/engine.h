@@ -54,6 +54,7 @@ struct DevicePlan {
   StageRec* d_stages = nullptr;
   void* d_ops = nullptr;
   void* fused = nullptr;       // fused-mode plan (owned by the fused module)
+  void* tc = nullptr;          // tensor-core pass plan (owned by tcpass.cu)
   int kmax = 0;                // tile bits the tiled plan was built for
   PlanStats stats;
 };

@@ -43,6 +43,7 @@
 #include "fusion.h"
 #include "kernels.h"
 #include "sv_device.cuh"
+#include "umma.cuh"
 
 namespace nqpu {
 
@@ -88,27 +89,11 @@ __device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t k) {
   return atom * (kRows * 128u) + (r >> 3) * 1024 + (r & 7) * 128 + ((chunk ^ (r & 7)) << 4) + within;
 }
 
-// Round-to-nearest TF32 (10 explicit mantissa bits): with hi = rn(x) and
-// lo = rn(x - hi), |x - hi - lo| <= 2^-24 |x| and the tensor core reads both
-// parts exactly.
-__device__ __forceinline__ float tf32_rn(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
-
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  // K-major, SWIZZLE_128B, SBO = 1024 B between 8-row groups, LBO unused (1),
-  // version 1 (sm_100), start address >> 4.
-  uint64_t d = 0;
-  d |= uint64_t((saddr >> 4) & 0x3FFF);
-  d |= uint64_t(1) << 16;
-  d |= uint64_t((1024 >> 4) & 0x3FFF) << 32;
-  d |= uint64_t(1) << 46;
-  d |= uint64_t(2) << 61;
-  return d;
-}
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) { return umma_desc_sw128(saddr); }
 
 // kind::tf32, D fp32, A/B tf32, both K-major, N = 64, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+static_assert(kIdesc == umma_idesc_tf32<128, 64>(), "instruction descriptor");
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
   asm volatile(
@@ -117,22 +102,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       :
       : "r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(addr), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t phase) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(addr), "r"(phase)
-      : "memory");
-  return ok != 0;
 }
 
 // Renormalisation: every launch writes the FP64 sum of |out|^2 of the tiles it

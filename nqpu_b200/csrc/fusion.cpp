@@ -13,7 +13,7 @@
 namespace nqpu {
 
 // Apply a lowered op to a 32-dim vector whose bit i is qubit q[i].
-static void apply_local(const Op& o, const int* q, cplx* v) {
+void fusion_apply_local(const Op& o, const int* q, cplx* v) {
   auto loc = [&](int qubit) {
     for (int i = 0; i < 5; ++i)
       if (q[i] == qubit) return i;
@@ -96,7 +96,7 @@ std::vector<FusedGate> fuse_ops(const std::vector<Op>& ops, int n) {
     for (int c = 0; c < 32; ++c) {
       cplx col[32];
       for (int r = 0; r < 32; ++r) col[r] = (r == c) ? cplx(1, 0) : cplx(0, 0);
-      for (int idx : take) apply_local(ops[idx], g.q, col);
+      for (int idx : take) fusion_apply_local(ops[idx], g.q, col);
       for (int r = 0; r < 32; ++r) g.u[r * 32 + c] = col[r];
     }
     g.n_ops = int(take.size());

@@ -16,4 +16,8 @@ struct FusedGate {
 // exactly 5 qubits (padded with the lowest unused qubits).  n >= 5.
 std::vector<FusedGate> fuse_ops(const std::vector<Op>& ops, int n);
 
+// Apply a lowered op to a 32-dim vector whose bit i is qubit q[i] (every
+// qubit of the op must be among q[0..4]); FP64, the engine's per-op arithmetic.
+void fusion_apply_local(const Op& o, const int* q, cplx* v);
+
 }  // namespace nqpu

@@ -1,0 +1,75 @@
+// Tensor-core pass mode: the plan data shared by the host planner
+// (tcplan.cpp), the sm_100a kernel (tcpass.cu) and the CPU emulator of the
+// kernel's index arithmetic (tests/tc_emulator.cpp).  Plain C++.
+//
+// One HBM pass streams the complex64 state through the SMs once.  A tile is
+// the 2^12 amplitudes that agree on every qubit outside the pass's tile-qubit
+// set Q (12 qubits; tile bit b <-> qubit qt[b]; tile bits 0..4 are qubits 0..4,
+// so a tile is 128 runs of 32 contiguous amplitudes).  The pass applies up to
+// kTcMaxUnitaries fused unitaries, each a dense 32x32 matrix on 5 of the tile
+// qubits, in order.  For unitary j the tile is a 128 x 32 complex matrix: row
+// bits = the 7 other tile bits (frow[i] = tile bit of row bit i), column bits =
+// the 5 fused tile bits (fcol[i]); the contraction is one tensor-core GEMM on
+// the real embedding (128 x 64 times 64 x 64, split TF32).  The tile never
+// returns to a natural layout between unitaries: the epilogue of unitary j
+// writes each amplitude straight to its place in unitary j+1's operand.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "sv_types.h"
+
+namespace nqpu {
+
+constexpr int kTcTileBits = 12;
+constexpr int kTcLowBits = 5;        // tile bits 0..4 = qubits 0..4
+constexpr int kTcMaxUnitaries = 2;   // per pass (their B operands stay in shared memory)
+constexpr int kTcMinQubits = 12;
+
+// Byte offset of element (row r, fp32 column k) in a K-major operand of
+// `rows` rows with the 128-byte swizzle: one K-atom (32 fp32 = 128 B per row)
+// every rows x 128 B, 8-row groups 1024 B apart, 16-byte chunks XOR-swizzled
+// with the row within its group.  GF(2)-linear in the bits of (r, k), since
+// its fields occupy disjoint bits.
+template <uint32_t kRows>
+inline constexpr uint32_t tc_sw128_off(uint32_t r, uint32_t k) {
+  return (k >> 5) * (kRows * 128u) + (r >> 3) * 1024u + (r & 7u) * 128u + ((((k & 31u) * 4u >> 4) ^ (r & 7u)) << 4) +
+         ((k & 31u) * 4u & 15u);
+}
+
+struct TcUnitaryRec {
+  int32_t frow[7];      // tile bit of row bit i
+  int32_t fcol[5];      // tile bit of column bit i
+  uint32_t boff[12];    // A-operand byte offset contributed by tile bit b in this layout
+  // Epilogue tables, per complex column c (tile part ct = deposit of c over fcol):
+  uint32_t xnext[32];   // operand byte offset of ct in the NEXT unitary's layout (not the last unitary)
+  uint64_t gcol[32];    // amplitude offset of ct (the last unitary: the HBM store)
+};
+
+struct TcPassRec {
+  int32_t m;                     // unitaries in this pass (1..kTcMaxUnitaries)
+  int32_t qt[kTcTileBits];       // qubit of tile bit b
+  int32_t n_out;                 // qubits outside Q (tile-id bits)
+  int32_t qout[kMaxQubits];      // qubit of tile-id bit j, ascending
+  int32_t pad;
+  TcUnitaryRec u[kTcMaxUnitaries];
+};
+
+struct TcPlan {
+  int n = 0;
+  std::vector<TcPassRec> passes;
+  // per pass, per unitary: 128 x 64 fp32 rows [n][k]: rows 0..63 = R_hi, rows
+  // 64..127 = R_lo of the real embedding R of U (R[2c'+a][2c+b] = [[Re,-Im],[Im,Re]][a][b] of U[c'][c])
+  std::vector<float> bmats;
+  // per pass, per unitary: the fused 32x32 complex unitary in FP64 (column index
+  // = fcol bits), for the CPU emulator and tests
+  std::vector<std::vector<cplx>> unitaries;
+  PlanStats stats;
+};
+
+constexpr size_t kTcBmatFloats = 128 * 64;
+
+// Plan a lowered op list for the tensor-core pass mode (complex64, n >= 12).
+bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err);
+
+}  // namespace nqpu
