@@ -302,15 +302,16 @@ def run_engine(args):
         ref_dtype = "c128" if args.dtype == "c64" else None
         if ref_dtype:
             sv128 = StateVector(n, ref_dtype)
+            mode128 = "tiled" if args.mode in ("tensor", "fused") else args.mode  # complex64-only modes
             t0 = time.perf_counter()
-            circ.execute(sv128, args.mode)
+            circ.execute(sv128, mode128)
             z128 = sv128.expectation_z_all()
             t128 = time.perf_counter() - t0
             f = sv.fidelity(sv128)
             extra["accuracy_vs_fp64"] = {"one_minus_F": 1.0 - f, "max_abs_dZ": float(np.abs(z_c64 - z128).max()),
                                          "tolerance": {"one_minus_F": 1e-5, "max_abs_dZ": 1e-5}}
-            extra["complex128_run"] = {"gates_per_s": G / t128, "seconds": t128,
-                                       "passes": circ.plan_stats(n, "c128", args.mode)["passes"]}
+            extra["complex128_run"] = {"gates_per_s": G / t128, "seconds": t128, "mode": mode128,
+                                       "passes": circ.plan_stats(n, "c128", mode128)["passes"]}
             # the same circuit through the per-gate path in complex128 (one
             # kernel per gate, no planner): a check of the planned engine at
             # the full size that does not rest on the planner

@@ -51,7 +51,10 @@ struct TcPassRec {
   int32_t qt[kTcTileBits];       // qubit of tile bit b
   int32_t n_out;                 // qubits outside Q (tile-id bits)
   int32_t qout[kMaxQubits];      // qubit of tile-id bit j, ascending
-  int32_t pad;
+  // loader: tile bit of loading-thread bit b (b = 0..8; bits 0..2 are tile
+  // bits 1..3, so 8 lanes read 128 contiguous bytes) and of load-step bit
+  // b - 9 (b = 9, 10); tile bit 0 is the pair inside each 16-byte load
+  int32_t lt[11];
   TcUnitaryRec u[kTcMaxUnitaries];
 };
 

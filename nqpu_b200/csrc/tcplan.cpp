@@ -21,10 +21,12 @@
 #include "tcpass.h"
 
 #include <algorithm>
-#include <array>
 #include <cmath>
 #include <cstring>
 #include <iterator>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
 
 #include "fusion.h"
 
@@ -45,19 +47,13 @@ float as_float(uint32_t b) {
   return f;
 }
 
-// Row choice of one layout: tile bits of row bits 0..4 (the remaining row bits
-// follow in ascending tile-bit order).
-struct RowChoice {
-  int lane[5];
-};
-
 // Byte offsets of the tile bits in a layout (frow / fcol given).
 void layout_offsets(const int* frow, const int* fcol, uint32_t* boff) {
   for (int i = 0; i < 7; ++i) boff[frow[i]] = tc_sw128_off<128>(1u << i, 0);
   for (int i = 0; i < 5; ++i) boff[fcol[i]] = tc_sw128_off<128>(0, 2u << i);
 }
 
-// GF(2) rank of 4-bit vectors.
+// GF(2) rank of 4-bit vectors (bits above 3 ignored).
 int rank4(const uint32_t* v, int cnt) {
   uint32_t basis[4] = {0, 0, 0, 0};
   int r = 0;
@@ -76,117 +72,169 @@ int rank4(const uint32_t* v, int cnt) {
   return r;
 }
 
-// Wavefronts of an 8-byte shared-memory store by a half warp whose lanes 0..15
-// run over the tile bits lb[0..3]: 2^(4 - rank) of the lanes' bank-slot bits
-// (address bits 3..6) in the target layout.
-int store_cost(const int* lb, const uint32_t* boff) {
+// Shared-memory wavefronts of one warp-wide store whose lanes run over the
+// tile bits lb[0..4], into a layout with byte offsets boff.  8-byte stores go
+// out a half warp (lane bits 0..3) at a time and are conflict-free when the
+// lanes' images in address bits 3..6 are independent; 16-byte stores go out a
+// quarter warp (lane bits 0..2) at a time and need address bits 4..6.  (The
+// kernel's ncu store-wavefront counts follow this rule.)
+int store_wavefronts(const int* lb, const uint32_t* boff, bool wide) {
   uint32_t v[4];
-  for (int i = 0; i < 4; ++i) v[i] = boff[lb[i]] >> 3;
-  return 1 << (4 - rank4(v, 4));
-}
-
-// 32-byte sectors of a warp's 8-byte HBM stores whose lanes run over the tile
-// bits lb[0..4] (tile bits 0 and 1 are qubits 0 and 1: 4 amplitudes per
-// sector), divided by the ideal 8.
-int hbm_cost(const int* lb) {
-  int low = 0;
-  for (int i = 0; i < 5; ++i) low += (lb[i] == 0 || lb[i] == 1) ? 1 : 0;
-  return 1 << (2 - low);
-}
-
-void fill_rows(const RowChoice& rc, uint32_t fmask, int* frow) {
-  int j = 0;
-  uint32_t used = fmask;
-  for (int i = 0; i < 5; ++i) {
-    frow[j++] = rc.lane[i];
-    used |= 1u << rc.lane[i];
+  if (wide) {
+    for (int i = 0; i < 3; ++i) v[i] = (boff[lb[i]] >> 4) & 7u;
+    return 4 << (3 - rank4(v, 3));
   }
-  for (int b = 0; b < kTcTileBits; ++b)
-    if (!((used >> b) & 1u)) frow[j++] = b;
+  for (int i = 0; i < 4; ++i) v[i] = boff[lb[i]] >> 3;
+  return 2 << (4 - rank4(v, 4));
 }
 
-// Candidate row choices of a layout: every ordered pick of 5 of the 7 row
-// tile bits reduces, for the costs above, to (set of rows 0..2, row 3, row 4);
-// the order inside rows 0..2 does not change any rank.
-std::vector<RowChoice> candidates(uint32_t fmask) {
-  int rows[7], nr = 0;
-  for (int b = 0; b < kTcTileBits; ++b)
-    if (!((fmask >> b) & 1u)) rows[nr++] = b;
-  std::vector<RowChoice> out;
-  for (int a = 0; a < 7; ++a)
-    for (int b = a + 1; b < 7; ++b)
-      for (int c = b + 1; c < 7; ++c)
-        for (int d = 0; d < 7; ++d) {
-          if (d == a || d == b || d == c) continue;
-          for (int e = 0; e < 7; ++e) {
-            if (e == a || e == b || e == c || e == d) continue;
-            RowChoice rc;
-            rc.lane[0] = rows[a];
-            rc.lane[1] = rows[b];
-            rc.lane[2] = rows[c];
-            rc.lane[3] = rows[d];
-            rc.lane[4] = rows[e];
-            out.push_back(rc);
-          }
-        }
-  return out;
+// Layout choice of a pass: column order and row order of every unitary's
+// operand, and the loader's map from thread / step bits to tile bits.
+struct LayoutCfg {
+  int fcol[kTcMaxUnitaries][5];
+  int frow[kTcMaxUnitaries][7];
+  int lt[11];
+};
+
+// Per-tile cost of a layout choice: shared-memory store wavefronts of the
+// loader and of the epilogues that feed the next unitary, plus a quarter unit
+// per 32-byte sector the last epilogue's HBM stores touch beyond the minimum
+// (partly written sectors still merge in L2 before they reach DRAM).
+int layout_cost(const LayoutCfg& c, int m, const int* qt) {
+  uint32_t boff[kTcMaxUnitaries][12];
+  for (int j = 0; j < m; ++j) layout_offsets(c.frow[j], c.fcol[j], boff[j]);
+  int cost = 0;
+  // loader: 16 warps x 4 steps, lanes over tile bits lt[0..4], hi and lo planes
+  if (c.fcol[0][0] == 0) cost += 64 * 2 * store_wavefronts(c.lt, boff[0], true);
+  else cost += 64 * 2 * 2 * store_wavefronts(c.lt, boff[0], false);
+  // epilogue: 16 warps x 8 columns (4 instructions of 16 bytes or 8 of 8)
+  for (int j = 0; j + 1 < m; ++j) {
+    const bool pair = c.fcol[j][0] == c.fcol[j + 1][0];
+    cost += 16 * (pair ? 4 : 8) * 2 * store_wavefronts(c.frow[j], boff[j + 1], pair);
+  }
+  // HBM: lanes over rows 0..4 of the last layout.  A 32-byte sector holds the
+  // 4 amplitudes that differ in qubits 0 and 1 (tile bits 0 and 1), so a warp
+  // touches 32 / 2^k sectors when k of those tile bits are lane bits; the
+  // minimum is 8 for 8-byte stores and 16 for 16-byte ones (qubit 0 is then a
+  // column bit and each lane writes a pair).
+  const int L = m - 1;
+  const bool wide = qt[c.fcol[L][0]] == 0;
+  int k = 0;
+  for (int i = 0; i < 5; ++i) k += (c.frow[L][i] == 0 || c.frow[L][i] == 1) ? 1 : 0;
+  const int ns = 32 >> k, ideal = wide ? 16 : 8;
+  cost += (8 * (wide ? 8 : 16) * (ns - ideal)) / 4;
+  return cost;
 }
 
-// Choose the row layouts of a pass's unitaries (fcol fixed) by dynamic
-// programming over the chain loader -> L0 -> L1 -> ... -> HBM.
+// Deterministic local search (best-improvement swaps from the sorted layout,
+// then seeded restarts until the cost reaches its lower bound) for the layout
+// choice of a pass.  The cost depends only on m and the fused tile-bit sets,
+// so results are kept in a process-wide cache keyed by those.
+std::mutex g_layout_mu;
+std::unordered_map<uint64_t, LayoutCfg> g_layout_cache;
+
 void choose_layouts(TcPassRec& P) {
   const int m = P.m;
-  std::vector<std::vector<RowChoice>> cand(static_cast<size_t>(m));
-  std::vector<std::vector<std::array<uint32_t, 12>>> offs(static_cast<size_t>(m));
+  uint64_t key = uint64_t(m);
   for (int j = 0; j < m; ++j) {
-    uint32_t fmask = 0;
-    for (int i = 0; i < 5; ++i) fmask |= 1u << P.u[j].fcol[i];
-    cand[size_t(j)] = candidates(fmask);
-    for (const RowChoice& rc : cand[size_t(j)]) {
-      int frow[7];
-      fill_rows(rc, fmask, frow);
-      std::array<uint32_t, 12> bo{};
-      layout_offsets(frow, P.u[j].fcol, bo.data());
-      offs[size_t(j)].push_back(bo);
+    uint64_t fm = 0;
+    for (int i = 0; i < 5; ++i) fm |= 1ull << P.u[j].fcol[i];
+    key |= fm << (4 + 12 * j);
+  }
+  auto apply = [&](const LayoutCfg& best) {
+    for (int j = 0; j < m; ++j) {
+      for (int i = 0; i < 5; ++i) P.u[j].fcol[i] = best.fcol[j][i];
+      for (int i = 0; i < 7; ++i) P.u[j].frow[i] = best.frow[j][i];
+    }
+    for (int b = 0; b < 11; ++b) P.lt[b] = best.lt[b];
+  };
+  {
+    std::lock_guard<std::mutex> lk(g_layout_mu);
+    auto it = g_layout_cache.find(key);
+    if (it != g_layout_cache.end()) {
+      apply(it->second);
+      return;
     }
   }
-  // the loader's half-warp lanes run over tile bits 1..4
-  const int loader_lanes[4] = {1, 2, 3, 4};
-  std::vector<std::vector<int>> best(static_cast<size_t>(m)), from(static_cast<size_t>(m));
+  LayoutCfg cur;
   for (int j = 0; j < m; ++j) {
-    const size_t nc = cand[size_t(j)].size();
-    best[size_t(j)].assign(nc, 1 << 30);
-    from[size_t(j)].assign(nc, -1);
-    for (size_t ci = 0; ci < nc; ++ci) {
-      const uint32_t* bo = offs[size_t(j)][ci].data();
-      if (j == 0) {
-        best[0][ci] = store_cost(loader_lanes, bo);
-        continue;
-      }
-      for (size_t pi = 0; pi < cand[size_t(j - 1)].size(); ++pi) {
-        const int c = best[size_t(j - 1)][pi] + store_cost(cand[size_t(j - 1)][pi].lane, bo);
-        if (c < best[size_t(j)][ci]) {
-          best[size_t(j)][ci] = c;
-          from[size_t(j)][ci] = int(pi);
+    for (int i = 0; i < 5; ++i) cur.fcol[j][i] = P.u[j].fcol[i];
+    uint32_t fm = 0;
+    for (int i = 0; i < 5; ++i) fm |= 1u << cur.fcol[j][i];
+    int r = 0;
+    for (int b = 0; b < kTcTileBits; ++b)
+      if (!((fm >> b) & 1u)) cur.frow[j][r++] = b;
+  }
+  for (int b = 0; b < 11; ++b) cur.lt[b] = b + 1;
+  uint64_t rng = 0x9E3779B97F4A7C15ull ^ (key * 0xD1B54A32D192ED03ull);  // a function of the cache key only
+  auto rnd = [&](int k) {
+    rng ^= rng << 13;
+    rng ^= rng >> 7;
+    rng ^= rng << 17;
+    return int(rng % uint64_t(k));
+  };
+  auto descend = [&](LayoutCfg& c) {
+    int cc = layout_cost(c, m, P.qt);
+    for (int iter = 0; iter < 64; ++iter) {
+      int best = cc;
+      LayoutCfg bc = c;
+      auto consider = [&](const LayoutCfg& t) {
+        const int v = layout_cost(t, m, P.qt);
+        if (v < best) {
+          best = v;
+          bc = t;
         }
+      };
+      for (int j = 0; j < m; ++j) {
+        for (int a = 0; a < 5; ++a)
+          for (int b = a + 1; b < 5; ++b) {
+            LayoutCfg t = c;
+            std::swap(t.fcol[j][a], t.fcol[j][b]);
+            consider(t);
+          }
+        for (int a = 0; a < 5; ++a)  // rows 5, 6 carry no cost: swaps among them are skipped
+          for (int b = a + 1; b < 7; ++b) {
+            LayoutCfg t = c;
+            std::swap(t.frow[j][a], t.frow[j][b]);
+            consider(t);
+          }
       }
+      for (int a = 3; a < 5; ++a)  // loader lane bits 3, 4 (lane bits 0..2 stay on qubits 1..3)
+        for (int b = 3; b < 11; ++b) {
+          if (a == b) continue;
+          LayoutCfg t = c;
+          std::swap(t.lt[a], t.lt[b]);
+          consider(t);
+        }
+      if (best >= cc) break;
+      c = bc;
+      cc = best;
+    }
+    return cc;
+  };
+  LayoutCfg best = cur;
+  int bestc = descend(best);
+  // lower bound: conflict-free stores (the loader's 16-byte or 8-byte stores
+  // move the same 512 wavefronts per tile, as does each epilogue into a next
+  // operand) and fully used HBM sectors
+  const int bound = 512 * m;
+  for (int restart = 0; restart < 40 && bestc > bound; ++restart) {
+    LayoutCfg t = cur;
+    for (int j = 0; j < m; ++j) {
+      for (int i = 4; i > 0; --i) std::swap(t.fcol[j][i], t.fcol[j][rnd(i + 1)]);
+      for (int i = 6; i > 0; --i) std::swap(t.frow[j][i], t.frow[j][rnd(i + 1)]);
+    }
+    for (int i = 10; i > 3; --i) std::swap(t.lt[i], t.lt[3 + rnd(i - 2)]);
+    const int v = descend(t);
+    if (v < bestc) {
+      bestc = v;
+      best = t;
     }
   }
-  // the last layout's epilogue stores to HBM (weighted as a global store)
-  int bi = 0, bc = 1 << 30;
-  for (size_t ci = 0; ci < cand[size_t(m - 1)].size(); ++ci) {
-    const int c = best[size_t(m - 1)][ci] + 2 * hbm_cost(cand[size_t(m - 1)][ci].lane);
-    if (c < bc) {
-      bc = c;
-      bi = int(ci);
-    }
-  }
-  for (int j = m - 1; j >= 0; --j) {
-    uint32_t fmask = 0;
-    for (int i = 0; i < 5; ++i) fmask |= 1u << P.u[j].fcol[i];
-    fill_rows(cand[size_t(j)][size_t(bi)], fmask, P.u[j].frow);
-    bi = from[size_t(j)][size_t(bi)];
-  }
+  apply(best);
+  std::lock_guard<std::mutex> lk(g_layout_mu);
+  if (g_layout_cache.size() >= 65536) g_layout_cache.clear();
+  g_layout_cache.emplace(key, best);
 }
 
 }  // namespace
@@ -202,6 +250,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     return false;
   }
   const uint64_t low = (1ull << kTcLowBits) - 1;
+  std::vector<std::vector<int>> cluster_ops;  // ops of each unitary, in pass order
   std::vector<int> remaining(ops.size());
   for (size_t i = 0; i < ops.size(); ++i) remaining[i] = int(i);
   while (!remaining.empty()) {
@@ -279,8 +328,21 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
       for (int b = 0; b < kTcTileBits; ++b)
         if ((F >> P.qt[b]) & 1ull) P.u[j].fcol[i++] = b;
     }
+    out->passes.push_back(P);
+    for (auto& cl : clusters) cluster_ops.push_back(std::move(cl.second));
+    out->stats.stages += uint64_t(P.m);
+    remaining.swap(rest);
+  }
+  // ---- per pass (independent, on host threads): layouts, offset tables,
+  // unitaries and their split real embeddings ----
+  const size_t np = out->passes.size();
+  std::vector<size_t> first_u(np + 1, 0);
+  for (size_t i = 0; i < np; ++i) first_u[i + 1] = first_u[i] + size_t(out->passes[i].m);
+  out->unitaries.assign(first_u[np], {});
+  out->bmats.assign(first_u[np] * kTcBmatFloats, 0.0f);
+  auto finish_pass = [&](size_t pi) {
+    TcPassRec& P = out->passes[pi];
     choose_layouts(P);
-    // ---- offset tables ----
     for (int j = 0; j < P.m; ++j) layout_offsets(P.u[j].frow, P.u[j].fcol, P.u[j].boff);
     for (int j = 0; j < P.m; ++j) {
       TcUnitaryRec& U = P.u[j];
@@ -296,20 +358,18 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
         U.gcol[c] = g;
       }
     }
-    // ---- unitaries and their split real embeddings ----
     for (int j = 0; j < P.m; ++j) {
+      const size_t ui = first_u[pi] + size_t(j);
       int q[5];
       for (int i = 0; i < 5; ++i) q[i] = P.qt[P.u[j].fcol[i]];
       std::vector<cplx> u(32 * 32, cplx(0, 0));
       for (int c = 0; c < 32; ++c) {
         cplx col[32];
         for (int r = 0; r < 32; ++r) col[r] = (r == c) ? cplx(1, 0) : cplx(0, 0);
-        for (int idx : clusters[size_t(j)].second) fusion_apply_local(ops[size_t(idx)], q, col);
+        for (int idx : cluster_ops[ui]) fusion_apply_local(ops[size_t(idx)], q, col);
         for (int r = 0; r < 32; ++r) u[size_t(r * 32 + c)] = col[r];
       }
-      const size_t base = out->bmats.size();
-      out->bmats.resize(base + kTcBmatFloats);
-      float* B = out->bmats.data() + base;
+      float* B = out->bmats.data() + ui * kTcBmatFloats;
       for (int co = 0; co < 32; ++co)
         for (int ci = 0; ci < 32; ++ci) {
           const cplx v = u[size_t(co * 32 + ci)];
@@ -323,11 +383,19 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
               B[(64 + nrow) * 64 + k] = lo;
             }
         }
-      out->unitaries.push_back(std::move(u));
+      out->unitaries[ui] = std::move(u);
     }
-    out->passes.push_back(P);
-    out->stats.stages += uint64_t(P.m);
-    remaining.swap(rest);
+  };
+  {
+    const size_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min(hw, std::max<size_t>(1, np / 4));
+    std::vector<std::thread> th;
+    auto work = [&](size_t t) {
+      for (size_t pi = t; pi < np; pi += nt) finish_pass(pi);
+    };
+    for (size_t t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
   }
   out->stats.passes = out->passes.size();
   out->stats.ops = ops.size();

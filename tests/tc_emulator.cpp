@@ -63,7 +63,8 @@ struct Operand {
 
 // Returns the number of passes (>= 0) or a negative error code:
 // -1 plan failed, -2 operand slot written twice / misaligned, -3 amplitude
-// written twice or not at all, -4 a 16-byte pairing condition does not hold.
+// written twice or not at all, -4 a 16-byte pairing condition does not hold,
+// -5 the loader's bit map is not a permutation with tile bits 1..3 first.
 extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, int split, int64_t* stats) {
   std::vector<GateRec> gates(static_cast<size_t>(ngates));
   for (int i = 0; i < ngates; ++i) {
@@ -106,16 +107,26 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
     }
     boff_base += size_t(m) * kTcBmatFloats;
     // loader tables (kernel: T->sol / T->sgl and the per-thread pol / pgl)
-    uint32_t sol[16];
-    uint64_t sgl[16];
-    for (int i = 0; i < 16; ++i) {
+    // (512 loading threads, 4 steps: thread bit b -> tile bit lt[b], step bit
+    // s -> tile bit lt[9 + s], tile bit 0 = the pair inside a 16-byte load)
+    uint32_t sol[4];
+    uint64_t sgl[4];
+    for (int i = 0; i < 4; ++i) {
       sol[i] = 0;
       sgl[i] = 0;
-      for (int s = 0; s < 4; ++s)
+      for (int s = 0; s < 2; ++s)
         if ((i >> s) & 1) {
-          sol[i] ^= P.u[0].boff[8 + s];
-          sgl[i] |= 1ull << P.qt[8 + s];
+          sol[i] ^= P.u[0].boff[P.lt[9 + s]];
+          sgl[i] |= 1ull << P.qt[P.lt[9 + s]];
         }
+    }
+    {
+      uint32_t seen = 1u;  // the loader map must be a permutation of tile bits 1..11
+      for (int b = 0; b < 11; ++b) {
+        if (P.lt[b] < 1 || P.lt[b] > 11 || ((seen >> P.lt[b]) & 1u)) return -5;
+        seen |= 1u << P.lt[b];
+      }
+      if (P.lt[0] != 1 || P.lt[1] != 2 || P.lt[2] != 3) return -5;
     }
     const uint32_t boff_h = P.u[0].boff[0];
     const bool load16 = boff_h == 8u;
@@ -127,15 +138,15 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
         if ((tile >> j) & 1ull) tb |= 1ull << P.qout[j];
       Operand A;
       A.clear();
-      for (uint32_t gt = 0; gt < 128; ++gt) {
+      for (uint32_t gt = 0; gt < 512; ++gt) {
         uint32_t pol = 0;
         uint64_t pgl = 0;
-        for (int b = 1; b <= 7; ++b)
-          if ((gt >> (b - 1)) & 1) {
-            pol ^= P.u[0].boff[b];
-            pgl |= 1ull << P.qt[b];
+        for (int b = 0; b < 9; ++b)
+          if ((gt >> b) & 1) {
+            pol ^= P.u[0].boff[P.lt[b]];
+            pgl |= 1ull << P.qt[P.lt[b]];
           }
-        for (int i = 0; i < 16; ++i) {
+        for (int i = 0; i < 4; ++i) {
           const uint64_t a = tb + pgl + sgl[i];  // even: the float4 of amplitudes a, a + 1
           if (a & 1ull) return -3;
           const uint32_t o = pol ^ sol[i];
