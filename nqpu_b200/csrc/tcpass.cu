@@ -1,32 +1,34 @@
 // Tensor-core pass mode (complex64): several fused 5-qubit unitaries per HBM
-// pass, each applied as a split-TF32 tcgen05 GEMM on a tile held in shared
-// memory (plan data and layouts in tcpass.h, planner in tcplan.cpp).
+// pass, each applied as a tcgen05 GEMM with split FP16 operands on a tile held
+// in shared memory (plan data and layouts in tcpass.h, planner in tcplan.cpp).
 //
-// Per pass, one persistent CTA per SM with two independent tile engines
-// ("groups" of sixteen warps).  A group owns an operand buffer (the tile as the
-// 128 x 64 fp32 A operand, hi and lo TF32 planes, K-major 128-byte swizzle) and
-// a 128-column TMEM accumulator, and runs its tiles through:
-//   load     4 coalesced 16-byte HBM loads per thread (a tile = 128 runs of
-//            32 amplitudes), scale by the renormalisation factor, split into
-//            TF32 hi/lo and store into the operand in unitary 0's layout;
-//   unitary  one elected thread issues 16 MMAs: D[:, 0:128] = A_hi [R_hi; R_lo]^T
-//            (N = 128, K = 64) then D[:, 0:64] += A_lo R_hi^T (N = 64), and
-//            commits them to the group's mbarrier (bounded wait);
-//   epilogue each thread reads a quarter of its row (TMEM lane) of D: warps
-//            w, w + 4, w + 8, w + 12 of a group share a lane quadrant and take
-//            8 columns each; it adds the two halves of D (out = A_hi R_hi +
-//            A_lo R_hi + A_hi R_lo) and either splits its 8 amplitudes straight
-//            into the next unitary's operand layout, or, after the last
-//            unitary, stores them to HBM.
-// While one group waits for its MMAs the other runs its loads and epilogues,
-// so the tensor pipe, shared memory and HBM overlap across the two tiles.
-// The B operands of the pass's unitaries stay in shared memory for the launch.
+// Per pass, one persistent CTA per SM with four independent tile engines of
+// eight warps.  An engine owns an operand buffer (the tile as the 128 x 64
+// FP16 A operand: hi and lo planes, K-major, 128-byte swizzle, 32 KB) and a
+// 128-column TMEM accumulator, and runs its tiles through:
+//   load     8 coalesced 16-byte HBM loads per thread (a tile = 128 runs of
+//            32 amplitudes), scale by s (a power of two, for the FP16 range)
+//            and the renormalisation factor, split x = hi + lo into FP16
+//            pairs and store them into the operand in unitary 0's layout;
+//   unitary  one elected thread issues 8 MMAs (K = 16): D[:, 0:128] =
+//            A_hi [B_hi; B_lo]^T (N = 128) then D[:, 0:64] += A_lo B_hi^T
+//            (N = 64), B = the real embedding of 16 U, and commits them to
+//            the engine's mbarrier (bounded wait);
+//   epilogue each thread reads half of its row (TMEM lane) of D: warps w and
+//            w + 4 of an engine share a lane quadrant and take 16 columns
+//            each; it forms out = (D[:, 0:64] + D[:, 64:128]) / 16 and either
+//            splits its amplitudes straight into the next unitary's operand
+//            layout, or, after the last unitary, stores out / s to HBM.
+// While one engine waits for its MMAs or its loads the other three run, so
+// the tensor pipe, shared memory and HBM overlap across four tiles.  The B
+// operands of the pass's unitaries stay in shared memory for the launch.
 //
 // Renormalisation: the first pass of a run records the FP64 norm of its input
 // (per-CTA partials) and every pass the norm of its output; each later pass
 // scales its input by sqrt(norm_in / norm_prev_out), so the norm drift of the
-// TF32 contractions is removed without an extra HBM pass and the state keeps
-// the norm it had when the run started.
+// split-precision contractions is removed without an extra HBM pass and the
+// state keeps the norm it had when the run started.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -42,16 +44,17 @@
 
 namespace nqpu {
 
-constexpr int kTcThreads = 1024;
-constexpr int kTcGroupThreads = 512;
-constexpr int kTcLoadSteps = 4;  // 16-byte loads per thread per tile
-constexpr uint32_t kTcAPlane = 128 * 64 * 4;         // 32 KB: 128 rows x 64 fp32
+constexpr int kTcEngines = 4;
+constexpr int kTcEngineThreads = 256;
+constexpr int kTcThreads = kTcEngines * kTcEngineThreads;
+constexpr int kTcLoadSteps = 1 << kTcLoadStepBits;   // 16-byte loads per thread per tile
+static_assert((1 << kTcLoadThreadBits) == kTcEngineThreads, "one loading thread per engine thread");
+static_assert(kTcLoadThreadBits + kTcLoadStepBits == kTcTileBits - 1, "loads cover the tile");
+constexpr uint32_t kTcAPlane = 128 * 128;            // 16 KB: 128 rows x 64 halves
 constexpr uint32_t kTcOpBytes = 2 * kTcAPlane;       // hi + lo planes
-constexpr uint32_t kTcBBytes = 128 * 64 * 4;         // [R_hi; R_lo]: 128 rows x 64 fp32
-constexpr uint32_t kTcAtom = 128 * 128;              // one K-atom (32 fp32) of 128 rows
+constexpr uint32_t kTcBBytes = 128 * 128;            // [B_hi; B_lo]: 128 rows x 64 halves
 constexpr uint32_t kTcWaitLimit = 1u << 22;          // bounded mbarrier polls
-constexpr uint32_t kTcTmemCols = 512;                // two groups x two 128-column accumulators
-static_assert(kTcThreads == 2 * kTcGroupThreads, "two tile engines per CTA");
+constexpr uint32_t kTcTmemCols = 512;                // four engines x one 128-column accumulator
 
 struct TcTables {
   uint32_t xnext[kTcMaxUnitaries][32];
@@ -60,37 +63,47 @@ struct TcTables {
   uint64_t sgl[kTcLoadSteps];  // loader: amplitude offset of load step i
 };
 
-constexpr size_t kTcSmem = 1024 /*alignment*/ + 2 * size_t(kTcOpBytes) + kTcMaxUnitaries * size_t(kTcBBytes) +
-                           sizeof(TcTables);
+constexpr size_t kTcSmem = 1024 /*alignment*/ + kTcEngines * size_t(kTcOpBytes) +
+                           kTcMaxUnitaries * size_t(kTcBBytes) + sizeof(TcTables);
 static_assert(kTcSmem <= 232448, "dynamic shared memory of one CTA");
 
-constexpr uint32_t kIdescN128 = umma_idesc_tf32<128, 128>();
-constexpr uint32_t kIdescN64 = umma_idesc_tf32<128, 64>();
+constexpr uint32_t kIdescN128 = umma_idesc_f16<128, 128>();
+constexpr uint32_t kIdescN64 = umma_idesc_f16<128, 64>();
 
-__device__ __forceinline__ void group_sync(int g) {
-  asm volatile("bar.sync %0, %1;\n" ::"r"(1 + g), "n"(kTcGroupThreads) : "memory");
+__device__ __forceinline__ void engine_sync(int e) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(1 + e), "n"(kTcEngineThreads) : "memory");
+}
+
+// FP16 hi/lo split of an (re, im) pair: hi = half(x), lo = half(x - hi)
+// (x - hi is exact in FP32; one packed FP32x2 FMA), as two packed half2 words.
+__device__ __forceinline__ void split_pair(float2 x, uint32_t& hi, uint32_t& lo) {
+  const __half2 h = __float22half2_rn(x);
+  const float2 r = __ffma2_rn(__half22float2(h), make_float2(-1.0f, -1.0f), x);
+  const __half2 l = __float22half2_rn(r);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_tc_pass(float* __restrict__ amp, const TcPassRec* __restrict__ pass, const float* __restrict__ bmats,
-              uint32_t n_tiles, const double* __restrict__ norm0, double* __restrict__ norm0_out,
-              const double* __restrict__ prev_norm, int n_prev, double* __restrict__ out_norm,
-              int* __restrict__ err) {
+    k_tc_pass(float* __restrict__ amp, const TcPassRec* __restrict__ pass, const uint16_t* __restrict__ bmats,
+              uint32_t n_tiles, float state_scale, const double* __restrict__ norm0,
+              double* __restrict__ norm0_out, const double* __restrict__ prev_norm, int n_prev,
+              double* __restrict__ out_norm, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw_s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_raw));
   unsigned char* base_p = smem_raw + ((1024 - (raw_s & 1023)) & 1023);
-  unsigned char* opbuf = base_p;                            // [2][hi | lo]
-  unsigned char* bbuf = base_p + 2 * kTcOpBytes;            // [m][128 rows x 64 fp32]
+  unsigned char* opbuf = base_p;                                    // [engine][hi | lo]
+  unsigned char* bbuf = base_p + kTcEngines * kTcOpBytes;           // [unitary][128 rows x 64 halves]
   TcTables* T = reinterpret_cast<TcTables*>(bbuf + kTcMaxUnitaries * kTcBBytes);
   __shared__ TcPassRec P;
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mbar[kTcEngines];
   __shared__ uint32_t tmem_holder;
-  __shared__ int s_abort[2];
+  __shared__ int s_abort[kTcEngines];
   __shared__ double s_red[2][kTcThreads / 32];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int g = tid >> 9, gt = tid & (kTcGroupThreads - 1);
-  const int q = warp & 3, cq = (warp >> 2) & 3;  // TMEM lane quadrant, column quarter
+  const int e = tid / kTcEngineThreads, et = tid % kTcEngineThreads;
+  const int q = warp & 3, ch = (warp >> 2) & 1;  // TMEM lane quadrant, column half
   const uint32_t row = uint32_t(32 * q + lane);  // this thread's operand row = its TMEM lane
 
   // ---- prologue: pass record, B operands, tables, barriers, TMEM ----
@@ -102,11 +115,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   const int m = P.m;
   for (int j = 0; j < m; ++j) {
-    const float4* bsrc = reinterpret_cast<const float4*>(bmats + size_t(j) * kTcBmatFloats);
+    // 8 halves (16 bytes) per copy: a 16-byte chunk of the swizzled row
+    const uint4* bsrc = reinterpret_cast<const uint4*>(bmats + size_t(j) * kTcBmatHalves);
     unsigned char* bdst = bbuf + j * kTcBBytes;
-    for (int e = tid; e < int(kTcBmatFloats / 4); e += kTcThreads) {
-      const uint32_t nrow = uint32_t(e) >> 4, k = (uint32_t(e) & 15u) * 4u;
-      *reinterpret_cast<float4*>(bdst + tc_sw128_off<128>(nrow, k)) = __ldg(bsrc + e);
+    for (int i = tid; i < int(kTcBmatHalves / 8); i += kTcThreads) {
+      const uint32_t nrow = uint32_t(i) >> 3, k = (uint32_t(i) & 7u) * 8u;
+      *reinterpret_cast<uint4*>(bdst + tc_sw128_off(nrow, k)) = __ldg(bsrc + i);
     }
   }
   for (int i = tid; i < m * 32; i += kTcThreads) {
@@ -116,19 +130,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (tid < kTcLoadSteps) {
     uint32_t o = 0;
     uint64_t a = 0;
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < kTcLoadStepBits; ++s)
       if ((tid >> s) & 1) {
-        o ^= P.u[0].boff[P.lt[9 + s]];
-        a |= 1ull << P.qt[P.lt[9 + s]];
+        o ^= P.u[0].boff[P.lt[kTcLoadThreadBits + s]];
+        a |= 1ull << P.qt[P.lt[kTcLoadThreadBits + s]];
       }
     T->sol[tid] = o;
     T->sgl[tid] = a;
   }
   const uint32_t mbar_s = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar[0]));
-  if (tid == 0) {
-    mbar_init(mbar_s, 1);
-    mbar_init(mbar_s + 8, 1);
-    s_abort[0] = s_abort[1] = 0;
+  if (tid < kTcEngines) {
+    mbar_init(mbar_s + 8u * uint32_t(tid), 1);
+    s_abort[tid] = 0;
   }
   if (warp == 0) {
     const uint32_t holder = static_cast<uint32_t>(__cvta_generic_to_shared(&tmem_holder));
@@ -143,41 +156,43 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
 
-  // renormalisation factor of this pass's input
-  float scale = 1.0f;
+  // renormalisation factor of this pass's input, times the operand scale s
+  float scale_in = state_scale;
   if (prev_norm && norm0) {
     double t0 = 0.0, tp = 0.0;
     for (int i = 0; i < n_prev; ++i) {
       t0 += norm0[i];
       tp += prev_norm[i];
     }
-    if (t0 > 0.0 && tp > 0.0) scale = float(sqrt(t0 / tp));
+    if (t0 > 0.0 && tp > 0.0) scale_in = float(double(state_scale) * sqrt(t0 / tp));
   }
+  const float mid_scale = 1.0f / kTcUScale;                       // exact: a power of two
+  const float out_scale = 1.0f / (kTcUScale * state_scale);       // exact: a power of two
 
   // ---- per-thread address parts ----
-  // loader: thread bit b of gt is tile bit lt[b], step bit s is tile bit
-  // lt[9 + s], and tile bit 0 is the pair inside each 16-byte load
+  // loader: thread bit b of et is tile bit lt[b], step bit s is tile bit
+  // lt[kTcLoadThreadBits + s], and tile bit 0 is the pair inside each 16-byte load
   uint32_t pol = 0;
   uint64_t pgl = 0;
-  for (int b = 0; b < 9; ++b)
-    if ((gt >> b) & 1) {
+  for (int b = 0; b < kTcLoadThreadBits; ++b)
+    if ((et >> b) & 1) {
       pol ^= P.u[0].boff[P.lt[b]];
       pgl |= 1ull << P.qt[P.lt[b]];
     }
   const uint32_t boff_h = P.u[0].boff[0];
-  const bool load16 = boff_h == 8u;  // tile bit 0 is column bit 0: (h = 0, 1) share a 16-byte chunk
+  const bool load_pair = boff_h == 4u;  // tile bit 0 is column bit 0: the two amplitudes are adjacent
   // epilogue of unitary j: row part of the thread's row (its TMEM lane)
   uint32_t ptn[kTcMaxUnitaries];
-  bool pair16[kTcMaxUnitaries];
+  bool pair[kTcMaxUnitaries];
   uint64_t pg = 0;
 #pragma unroll
   for (int j = 0; j < kTcMaxUnitaries; ++j) {
     ptn[j] = 0;
-    pair16[j] = false;
+    pair[j] = false;
     if (j + 1 < m) {
       for (int i = 0; i < 7; ++i)
         if ((row >> i) & 1u) ptn[j] ^= P.u[j + 1].boff[P.u[j].frow[i]];
-      pair16[j] = P.u[j + 1].boff[P.u[j].fcol[0]] == 8u;
+      pair[j] = P.u[j + 1].boff[P.u[j].fcol[0]] == 4u;
     } else if (j + 1 == m) {
       for (int i = 0; i < 7; ++i)
         if ((row >> i) & 1u) pg |= 1ull << P.qt[P.u[j].frow[i]];
@@ -185,221 +200,164 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   const bool store16 = P.qt[P.u[m - 1].fcol[0]] == 0;  // qubit 0 is column bit 0 of the last layout
 
-  const uint32_t ahi_s = static_cast<uint32_t>(__cvta_generic_to_shared(opbuf)) + uint32_t(g) * kTcOpBytes;
+  const uint32_t ahi_s = static_cast<uint32_t>(__cvta_generic_to_shared(opbuf)) + uint32_t(e) * kTcOpBytes;
   const uint32_t alo_s = ahi_s + kTcAPlane;
   const uint32_t b_s = static_cast<uint32_t>(__cvta_generic_to_shared(bbuf));
-  const uint32_t my_mbar = mbar_s + 8u * uint32_t(g);
+  const uint32_t my_mbar = mbar_s + 8u * uint32_t(e);
+  const uint32_t acc = tmem + 128u * uint32_t(e);
+  const uint32_t lanes = acc + (uint32_t(q * 32) << 16) + 32u * uint32_t(ch);
 
-  // split (re, im) pairs into the hi and lo operand planes at byte offset o
-  auto put2 = [&](uint32_t o, float re, float im) {
-    const float hr = tf32_rn(re), hi = tf32_rn(im);
-    sts_v2(ahi_s + o, hr, hi);
-    sts_v2(alo_s + o, tf32_rn(re - hr), tf32_rn(im - hi));
-  };
-  auto put4 = [&](uint32_t o, float4 x) {
-    const float4 h = make_float4(tf32_rn(x.x), tf32_rn(x.y), tf32_rn(x.z), tf32_rn(x.w));
-    sts_v4(ahi_s + o, h.x, h.y, h.z, h.w);
-    sts_v4(alo_s + o, tf32_rn(x.x - h.x), tf32_rn(x.y - h.y), tf32_rn(x.z - h.z), tf32_rn(x.w - h.w));
-  };
   auto tile_base_of = [&](uint32_t tile) {
     const uint64_t mine = (lane < P.n_out && ((tile >> lane) & 1u)) ? (1ull << P.qout[lane]) : 0ull;
     const uint32_t lo = __reduce_or_sync(0xffffffffu, uint32_t(mine));
     const uint32_t hi = __reduce_or_sync(0xffffffffu, uint32_t(mine >> 32));
     return uint64_t(lo) | (uint64_t(hi) << 32);
   };
+  // split an amplitude (or two adjacent ones) into the hi / lo planes at byte offset o
+  auto put1 = [&](uint32_t o, float2 x) {
+    uint32_t h, l;
+    split_pair(x, h, l);
+    sts_b32(ahi_s + o, h);
+    sts_b32(alo_s + o, l);
+  };
+  auto put2 = [&](uint32_t o, float2 x0, float2 x1) {
+    uint32_t h0, l0, h1, l1;
+    split_pair(x0, h0, l0);
+    split_pair(x1, h1, l1);
+    sts_v2_b32(ahi_s + o, h0, h1);
+    sts_v2_b32(alo_s + o, l0, l1);
+  };
+  auto engine_barrier = [&]() {
+    tc_fence_before();
+    engine_sync(e);
+    tc_fence_after();
+  };
 
   double norm_in = 0.0, norm_out = 0.0;
-  uint32_t phase = 0;   // parity of the group's mbarrier phase to wait for
-  uint32_t batches = 0; // MMA batches issued by this group (accumulator = batches & 1)
-  const uint32_t stride = 2u * gridDim.x;
-
-  // HBM -> registers (16-byte loads; tile bit 0 is the pair inside each)
-  auto load_tile = [&](uint64_t tb, float4 (&v)[kTcLoadSteps]) {
-    const float4* src = reinterpret_cast<const float4*>(amp) + ((tb + pgl) >> 1);
+  uint32_t phase = 0;  // parity of the engine's mbarrier phase to wait for
+  const uint32_t stride = uint32_t(kTcEngines) * gridDim.x;
+  for (uint32_t tile = uint32_t(kTcEngines) * blockIdx.x + uint32_t(e); tile < n_tiles; tile += stride) {
+    const uint64_t tb = tile_base_of(tile);
+    // ---- load, scale, split into unitary 0's operand ----
+    {
+      // pull this engine's next tile into L2 first (no registers held), so its
+      // loads will meet L2 rather than DRAM latency
+      if (tile + stride < n_tiles) {
+        const float4* nsrc = reinterpret_cast<const float4*>(amp) + ((tile_base_of(tile + stride) + pgl) >> 1);
 #pragma unroll
-    for (int i = 0; i < kTcLoadSteps; ++i) v[i] = __ldcs(src + (T->sgl[i] >> 1));
-  };
-  // registers -> unitary 0's operand: renormalise, split, store
-  auto split_tile = [&](const float4 (&v)[kTcLoadSteps]) {
-    float tile_in = 0.0f;  // this thread's 8 amplitudes: an FP32 partial, then FP64 across tiles
-#pragma unroll
-    for (int i = 0; i < kTcLoadSteps; ++i) {
-      float4 x = v[i];
-      if (norm0_out) tile_in += x.x * x.x + x.y * x.y + x.z * x.z + x.w * x.w;
-      x.x *= scale;
-      x.y *= scale;
-      x.z *= scale;
-      x.w *= scale;
-      const uint32_t o = pol ^ T->sol[i];
-      if (load16) {
-        put4(o, x);
-      } else {
-        put2(o, x.x, x.y);
-        put2(o ^ boff_h, x.z, x.w);
+        for (int i = 0; i < kTcLoadSteps; ++i) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(nsrc + (T->sgl[i] >> 1)));
       }
-    }
-    if (norm0_out) norm_in += double(tile_in);
-    fence_proxy_async_smem();
-  };
-  // one elected thread: unitary j's 16 MMAs into the next free accumulator.
-  // The descriptors differ only in their start-address field (address >> 4,
-  // bits 0..13, which no offset here carries out of), so each is a base
-  // descriptor plus a compile-time constant.
-  auto issue_unitary = [&](int j) -> uint32_t {
-    const uint32_t acc = tmem + 256u * uint32_t(g) + 128u * (batches & 1u);
-    if (gt == 0) {
-      const uint64_t dhi = umma_desc_sw128(ahi_s), dlo = umma_desc_sw128(alo_s);
-      const uint64_t dbj = umma_desc_sw128(b_s + uint32_t(j) * kTcBBytes);
+      float4 v[kTcLoadSteps];
+      const float4* src = reinterpret_cast<const float4*>(amp) + ((tb + pgl) >> 1);
 #pragma unroll
-      for (int kk = 0; kk < 8; ++kk) {
-        const uint64_t off = (uint64_t(kk >> 2) * kTcAtom + uint64_t(kk & 3) * 32u) >> 4;
-        umma_tf32(acc, dhi + off, dbj + off, kIdescN128, kk > 0 ? 1u : 0u);
-      }
+      for (int i = 0; i < kTcLoadSteps; ++i) v[i] = __ldcs(src + (T->sgl[i] >> 1));
+      const float2 s2 = make_float2(scale_in, scale_in);
+      float2 nin = make_float2(0.0f, 0.0f);  // FP32 partials over this thread's amplitudes, FP64 across tiles
 #pragma unroll
-      for (int kk = 0; kk < 8; ++kk) {
-        const uint64_t off = (uint64_t(kk >> 2) * kTcAtom + uint64_t(kk & 3) * 32u) >> 4;
-        umma_tf32(acc, dlo + off, dbj + off, kIdescN64, 1u);
-      }
-      umma_commit(my_mbar);
-    }
-    ++batches;
-    return acc;
-  };
-  auto group_barrier = [&]() {
-    tc_fence_before();
-    group_sync(g);
-    tc_fence_after();
-  };
-  // bounded wait for the group's outstanding MMA batch; false: give up
-  auto wait_unitary = [&]() -> bool {
-    uint32_t it = 0;
-    bool done = false;
-    while (!(done = mbar_try_wait(my_mbar, phase)) && ++it < kTcWaitLimit) {
-    }
-    if (!done) {
-      atomicExch(err, 1);
-      s_abort[g] = 1;
-      // the MMAs may still be running: one more bounded wait before this
-      // group stops and the CTA's normal exit frees the accumulators
-      for (uint32_t w = 0; w < 4 * kTcWaitLimit && !mbar_try_wait(my_mbar, phase); ++w) {
-      }
-    }
-    group_sync(g);
-    phase ^= 1u;
-    tc_fence_after();
-    return s_abort[g] == 0;
-  };
-  // epilogue of unitary j (not the last): accumulator -> next operand layout
-  auto epilogue_mid = [&](int j, uint32_t acc) {
-    uint32_t my_ptn = 0;
-    bool my_pair = false;
-#pragma unroll
-    for (int jj = 0; jj < kTcMaxUnitaries; ++jj)
-      if (jj == j) {
-        my_ptn = ptn[jj];
-        my_pair = pair16[jj];
-      }
-    const uint32_t lanes = acc + (uint32_t(q * 32) << 16) + 16u * uint32_t(cq);
-#pragma unroll
-    for (int part = 0; part < 2; ++part) {
-      uint32_t rh[8], rl[8];
-      tmem_ld8(lanes + 8u * uint32_t(part), rh);
-      tmem_ld8(lanes + 64u + 8u * uint32_t(part), rl);
-      tmem_ld_wait();
-#pragma unroll
-      for (int cc = 0; cc < 4; cc += 2) {
-        const int c = 8 * cq + 4 * part + cc;
-        const float re0 = __uint_as_float(rh[2 * cc]) + __uint_as_float(rl[2 * cc]);
-        const float im0 = __uint_as_float(rh[2 * cc + 1]) + __uint_as_float(rl[2 * cc + 1]);
-        const float re1 = __uint_as_float(rh[2 * cc + 2]) + __uint_as_float(rl[2 * cc + 2]);
-        const float im1 = __uint_as_float(rh[2 * cc + 3]) + __uint_as_float(rl[2 * cc + 3]);
-        const uint32_t o0 = my_ptn ^ T->xnext[j][c];
-        if (my_pair) {
-          put4(o0, make_float4(re0, im0, re1, im1));
+      for (int i = 0; i < kTcLoadSteps; ++i) {
+        const float2 x0 = make_float2(v[i].x, v[i].y), x1 = make_float2(v[i].z, v[i].w);
+        if (norm0_out) nin = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nin));
+        const uint32_t o = pol ^ T->sol[i];
+        if (load_pair) {
+          put2(o, __fmul2_rn(x0, s2), __fmul2_rn(x1, s2));
         } else {
-          put2(o0, re0, im0);
-          put2(my_ptn ^ T->xnext[j][c + 1], re1, im1);
+          put1(o, __fmul2_rn(x0, s2));
+          put1(o ^ boff_h, __fmul2_rn(x1, s2));
         }
       }
+      if (norm0_out) norm_in += double(nin.x) + double(nin.y);
     }
     fence_proxy_async_smem();
-  };
-  // epilogue of the last unitary: accumulator -> HBM, FP64 norm of the output
-  auto epilogue_last = [&](uint64_t tb, uint32_t acc) {
-    const int j = m - 1;
-    const uint32_t lanes = acc + (uint32_t(q * 32) << 16) + 16u * uint32_t(cq);
-    float2* out = reinterpret_cast<float2*>(amp) + (tb + pg);
-    float tile_out = 0.0f;  // FP32 partial over this thread's 8 amplitudes
+    engine_barrier();
+    bool aborted = false;
+    for (int j = 0; j < m; ++j) {
+      // ---- unitary j on the tensor cores: 8 MMAs of K = 16 ----
+      if (et == 0) {
+        // the descriptors differ only in their start-address field (address
+        // >> 4), which these offsets do not carry out of
+        const uint64_t dhi = umma_desc_sw128(ahi_s), dlo = umma_desc_sw128(alo_s);
+        const uint64_t dbj = umma_desc_sw128(b_s + uint32_t(j) * kTcBBytes);
 #pragma unroll
-    for (int part = 0; part < 2; ++part) {
-      uint32_t rh[8], rl[8];
-      tmem_ld8(lanes + 8u * uint32_t(part), rh);
-      tmem_ld8(lanes + 64u + 8u * uint32_t(part), rl);
-      tmem_ld_wait();
+        for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dhi + 2u * kk, dbj + 2u * kk, kIdescN128, kk > 0 ? 1u : 0u);
 #pragma unroll
-      for (int cc = 0; cc < 4; cc += 2) {
-        const int c = 8 * cq + 4 * part + cc;
-        const float re0 = __uint_as_float(rh[2 * cc]) + __uint_as_float(rl[2 * cc]);
-        const float im0 = __uint_as_float(rh[2 * cc + 1]) + __uint_as_float(rl[2 * cc + 1]);
-        const float re1 = __uint_as_float(rh[2 * cc + 2]) + __uint_as_float(rl[2 * cc + 2]);
-        const float im1 = __uint_as_float(rh[2 * cc + 3]) + __uint_as_float(rl[2 * cc + 3]);
-        tile_out += re0 * re0 + im0 * im0 + re1 * re1 + im1 * im1;
-        if (store16) {
-          __stcs(reinterpret_cast<float4*>(out + T->gcol[j][c]), make_float4(re0, im0, re1, im1));
-        } else {
-          __stcs(out + T->gcol[j][c], make_float2(re0, im0));
-          __stcs(out + T->gcol[j][c + 1], make_float2(re1, im1));
+        for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dlo + 2u * kk, dbj + 2u * kk, kIdescN64, 1u);
+        umma_commit(my_mbar);
+      }
+      {
+        uint32_t it = 0;
+        bool done = false;
+        while (!(done = mbar_try_wait(my_mbar, phase)) && ++it < kTcWaitLimit) {
         }
-      }
-    }
-    norm_out += double(tile_out);
-  };
-
-  // Software pipeline over the group's tiles t0, t1, ...: the HBM loads of
-  // tile t+1 are issued as tile t's first MMAs start and land in registers
-  // while tile t runs (no further prefetch: more loads in flight only throttle
-  // the load-store unit); when tile t's last MMAs are done the operand buffer is
-  // free, so tile t+1 is split into it and its first MMAs run (into the other
-  // accumulator) while tile t's last epilogue drains to HBM.
-  uint32_t tile = 2u * blockIdx.x + uint32_t(g);
-  if (tile < n_tiles) {
-    float4 v[kTcLoadSteps];
-    uint64_t tb = tile_base_of(tile);
-    load_tile(tb, v);
-    split_tile(v);
-    group_barrier();
-    uint32_t acc = issue_unitary(0);
-    for (;;) {
-      const uint32_t next = tile + stride;
-      const bool has_next = next < n_tiles;
-      uint64_t ntb = 0;
-      if (has_next) {
-        ntb = tile_base_of(next);
-        load_tile(ntb, v);  // registers free since the split of `tile`
-      }
-      bool ok = true;
-      for (int j = 0; j < m && ok; ++j) {
-        ok = wait_unitary();
-        if (!ok) break;
-        if (j + 1 < m) {
-          epilogue_mid(j, acc);  // writes the operand the finished MMAs read
-          group_barrier();
-          acc = issue_unitary(j + 1);
-        } else {
-          const uint32_t acc_last = acc;
-          if (has_next) {
-            split_tile(v);  // the operand is free: tile `next` goes in
-            group_barrier();
-            acc = issue_unitary(0);  // into the other accumulator
+        if (!done) {
+          atomicExch(err, 1);
+          s_abort[e] = 1;
+          // the MMAs may still be running: one more bounded wait before this
+          // engine stops and the CTA's normal exit frees the accumulators
+          for (uint32_t w = 0; w < 4 * kTcWaitLimit && !mbar_try_wait(my_mbar, phase); ++w) {
           }
-          epilogue_last(tb, acc_last);
-          group_barrier();  // acc_last drained before an MMA reuses it
+        }
+        engine_sync(e);
+        phase ^= 1u;
+        if (s_abort[e]) {
+          aborted = true;
+          break;
         }
       }
-      if (!ok || !has_next) break;
-      tile = next;
-      tb = ntb;
+      tc_fence_after();
+      // ---- epilogue of unitary j ----
+      const bool last = j + 1 == m;
+      uint32_t my_ptn = 0;
+      bool my_pair = false;
+#pragma unroll
+      for (int jj = 0; jj < kTcMaxUnitaries; ++jj)
+        if (jj == j) {
+          my_ptn = ptn[jj];
+          my_pair = pair[jj];
+        }
+      float2* out = reinterpret_cast<float2*>(amp) + (tb + pg);
+      float2 nout = make_float2(0.0f, 0.0f);
+      const float scv = last ? out_scale : mid_scale;
+      const float2 sc = make_float2(scv, scv);
+#pragma unroll
+      for (int part = 0; part < 4; ++part) {
+        uint32_t rh[8], rl[8];
+        tmem_ld8(lanes + 8u * uint32_t(part), rh);
+        tmem_ld8(lanes + 64u + 8u * uint32_t(part), rl);
+        tmem_ld_wait();
+#pragma unroll
+        for (int cc = 0; cc < 4; cc += 2) {
+          const int c = 16 * ch + 4 * part + cc;
+          // out = (D[:, 0:64] + D[:, 64:128]) * scale, packed (re, im)
+          const float2 x0 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[2 * cc]), __uint_as_float(rh[2 * cc + 1])),
+                                                  make_float2(__uint_as_float(rl[2 * cc]), __uint_as_float(rl[2 * cc + 1]))),
+                                       sc);
+          const float2 x1 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[2 * cc + 2]), __uint_as_float(rh[2 * cc + 3])),
+                                                  make_float2(__uint_as_float(rl[2 * cc + 2]), __uint_as_float(rl[2 * cc + 3]))),
+                                       sc);
+          if (!last) {
+            const uint32_t o0 = my_ptn ^ T->xnext[j][c];
+            if (my_pair) {
+              put2(o0, x0, x1);
+            } else {
+              put1(o0, x0);
+              put1(my_ptn ^ T->xnext[j][c + 1], x1);
+            }
+          } else {
+            nout = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nout));
+            if (store16) {
+              __stcs(reinterpret_cast<float4*>(out + T->gcol[j][c]), make_float4(x0.x, x0.y, x1.x, x1.y));
+            } else {
+              __stcs(out + T->gcol[j][c], x0);
+              __stcs(out + T->gcol[j][c + 1], x1);
+            }
+          }
+        }
+      }
+      if (last) norm_out += double(nout.x) + double(nout.y);
+      else fence_proxy_async_smem();
+      engine_barrier();  // the accumulator is drained before the next MMAs overwrite it
     }
+    if (aborted) break;
   }
 
   // ---- per-CTA FP64 norm partials (fixed-order reduction), teardown ----
@@ -433,9 +391,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ---------------------------------------------------------------------------
 struct TcPlanImpl {
   TcPlan plan;
-  std::vector<size_t> bmat_off;   // first B-operand float of each pass
+  std::vector<size_t> bmat_off;   // first B-operand half of each pass
   TcPassRec* d_passes = nullptr;
-  float* d_bmats = nullptr;
+  uint16_t* d_bmats = nullptr;
   double* d_norm = nullptr;       // [norm0 | out ping | out pong], `slots` doubles each
   int slots = 0;
   int* d_err = nullptr;
@@ -453,16 +411,17 @@ bool tc_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, Pla
   size_t off = 0;
   for (const TcPassRec& P : p->plan.passes) {
     p->bmat_off.push_back(off);
-    off += size_t(P.m) * kTcBmatFloats;
+    off += size_t(P.m) * kTcBmatHalves;
   }
   const size_t np = std::max<size_t>(1, p->plan.passes.size());
   bool ok = cudaMalloc(reinterpret_cast<void**>(&p->d_passes), np * sizeof(TcPassRec)) == cudaSuccess;
-  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_bmats), std::max<size_t>(1, off) * sizeof(float)) == cudaSuccess;
+  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_bmats), std::max<size_t>(8, off) * sizeof(uint16_t)) ==
+                 cudaSuccess;
   if (ok && !p->plan.passes.empty())
     ok = cudaMemcpy(p->d_passes, p->plan.passes.data(), p->plan.passes.size() * sizeof(TcPassRec),
                     cudaMemcpyHostToDevice) == cudaSuccess;
   if (ok && off)
-    ok = cudaMemcpy(p->d_bmats, p->plan.bmats.data(), off * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = cudaMemcpy(p->d_bmats, p->plan.bmats.data(), off * sizeof(uint16_t), cudaMemcpyHostToDevice) == cudaSuccess;
   p->slots = device_sms();
   ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_norm), sizeof(double) * 3 * size_t(p->slots)) == cudaSuccess;
   ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_err), sizeof(int)) == cudaSuccess;
@@ -506,15 +465,16 @@ cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
   e = attr.get(dev, [] { return cudaFuncSetAttribute(k_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)); },
                cudaErrorInvalidDevice);
   if (e != cudaSuccess) return e;
-  const uint64_t n_tiles = 1ull << (p->plan.n - kTcTileBits);
-  const unsigned grid = unsigned(std::min<uint64_t>((n_tiles + 1) / 2, uint64_t(p->slots)));
+  const uint32_t n_tiles = uint32_t(1) << (p->plan.n - kTcTileBits);
+  const unsigned grid =
+      unsigned(std::min<uint64_t>((uint64_t(n_tiles) + kTcEngines - 1) / kTcEngines, uint64_t(p->slots)));
   double* norm0 = p->d_norm;
   for (size_t i = 0; i < p->plan.passes.size(); ++i) {
     double* outn = p->d_norm + (1 + (i & 1)) * size_t(p->slots);
     const double* prevn = i ? p->d_norm + (1 + ((i + 1) & 1)) * size_t(p->slots) : nullptr;
     k_tc_pass<<<grid, kTcThreads, kTcSmem, s->stream>>>(
-        static_cast<float*>(s->amp), p->d_passes + i, p->d_bmats + p->bmat_off[i], uint32_t(n_tiles), i ? norm0 : nullptr,
-        i ? nullptr : norm0, prevn, int(grid), outn, p->d_err);
+        static_cast<float*>(s->amp), p->d_passes + i, p->d_bmats + p->bmat_off[i], n_tiles, p->plan.state_scale,
+        i ? norm0 : nullptr, i ? nullptr : norm0, prevn, int(grid), outn, p->d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (events) {
       cudaEvent_t ev;

@@ -10,9 +10,11 @@
 // qubits, in order.  For unitary j the tile is a 128 x 32 complex matrix: row
 // bits = the 7 other tile bits (frow[i] = tile bit of row bit i), column bits =
 // the 5 fused tile bits (fcol[i]); the contraction is one tensor-core GEMM on
-// the real embedding (128 x 64 times 64 x 64, split TF32).  The tile never
-// returns to a natural layout between unitaries: the epilogue of unitary j
-// writes each amplitude straight to its place in unitary j+1's operand.
+// the real embedding (128 x 64 times 64 x 64).  Operands are FP16 hi/lo pairs
+// (x = hi + lo, 22 significant bits) of the amplitudes scaled by a power of two
+// and of 16 U, accumulated in FP32.  The tile never returns to a natural layout
+// between unitaries: the epilogue of unitary j writes each amplitude straight
+// to its place in unitary j+1's operand.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -23,18 +25,22 @@ namespace nqpu {
 
 constexpr int kTcTileBits = 12;
 constexpr int kTcLowBits = 5;        // tile bits 0..4 = qubits 0..4
-constexpr int kTcMaxUnitaries = 2;   // per pass (their B operands stay in shared memory)
+constexpr int kTcMaxUnitaries = 3;   // per pass (their B operands stay in shared memory)
 constexpr int kTcMinQubits = 12;
+constexpr int kTcLoadThreadBits = 8; // loading threads per tile engine: 256
+constexpr int kTcLoadStepBits = 3;   // 16-byte loads per thread: 8
+// The unitaries are stored as 16 U (entries up to 16 in magnitude keep their
+// small entries clear of the FP16 subnormal range); epilogues divide by 16.
+constexpr float kTcUScale = 16.0f;
 
-// Byte offset of element (row r, fp32 column k) in a K-major operand of
-// `rows` rows with the 128-byte swizzle: one K-atom (32 fp32 = 128 B per row)
-// every rows x 128 B, 8-row groups 1024 B apart, 16-byte chunks XOR-swizzled
-// with the row within its group.  GF(2)-linear in the bits of (r, k), since
-// its fields occupy disjoint bits.
-template <uint32_t kRows>
+// Byte offset of element (row r, 16-bit column k < 64) in a K-major operand
+// with the 128-byte swizzle: 128 bytes per row (one K-atom of 64 halves),
+// 8-row groups 1024 B apart, 16-byte chunks XOR-swizzled with the row within
+// its group.  GF(2)-linear in the bits of (r, k), since its fields occupy
+// disjoint bits.  Complex column c of a row is the half pair (re, im) at
+// k = 2c, 2c + 1: 4 bytes.
 inline constexpr uint32_t tc_sw128_off(uint32_t r, uint32_t k) {
-  return (k >> 5) * (kRows * 128u) + (r >> 3) * 1024u + (r & 7u) * 128u + ((((k & 31u) * 4u >> 4) ^ (r & 7u)) << 4) +
-         ((k & 31u) * 4u & 15u);
+  return (r >> 3) * 1024u + (r & 7u) * 128u + ((((k & 63u) * 2u >> 4) ^ (r & 7u)) << 4) + ((k & 63u) * 2u & 15u);
 }
 
 struct TcUnitaryRec {
@@ -51,26 +57,37 @@ struct TcPassRec {
   int32_t qt[kTcTileBits];       // qubit of tile bit b
   int32_t n_out;                 // qubits outside Q (tile-id bits)
   int32_t qout[kMaxQubits];      // qubit of tile-id bit j, ascending
-  // loader: tile bit of loading-thread bit b (b = 0..8; bits 0..2 are tile
-  // bits 1..3, so 8 lanes read 128 contiguous bytes) and of load-step bit
-  // b - 9 (b = 9, 10); tile bit 0 is the pair inside each 16-byte load
+  // loader: tile bit of loading-thread bit b (b < kTcLoadThreadBits; bits 0..2
+  // are tile bits 1..3, so 8 lanes read 128 contiguous bytes) and of load-step
+  // bit b - kTcLoadThreadBits; tile bit 0 is the pair inside each 16-byte load
   int32_t lt[11];
   TcUnitaryRec u[kTcMaxUnitaries];
 };
 
 struct TcPlan {
   int n = 0;
+  float state_scale = 1.0f;      // amplitudes enter the operands multiplied by this power of two
   std::vector<TcPassRec> passes;
-  // per pass, per unitary: 128 x 64 fp32 rows [n][k]: rows 0..63 = R_hi, rows
-  // 64..127 = R_lo of the real embedding R of U (R[2c'+a][2c+b] = [[Re,-Im],[Im,Re]][a][b] of U[c'][c])
-  std::vector<float> bmats;
+  // per pass, per unitary: 128 x 64 halves (as uint16 bit patterns), rows [n][k]:
+  // rows 0..63 = hi, rows 64..127 = lo of the real embedding R of 16 U
+  // (R[2c'+a][2c+b] = [[Re,-Im],[Im,Re]][a][b] of 16 U[c'][c])
+  std::vector<uint16_t> bmats;
   // per pass, per unitary: the fused 32x32 complex unitary in FP64 (column index
   // = fcol bits), for the CPU emulator and tests
   std::vector<std::vector<cplx>> unitaries;
   PlanStats stats;
 };
 
-constexpr size_t kTcBmatFloats = 128 * 64;
+constexpr size_t kTcBmatHalves = 128 * 64;
+
+// IEEE binary16 round-to-nearest-even of a float (host side), and back.
+uint16_t tc_half_bits(float x);
+float tc_half_value(uint16_t h);
+
+// Power-of-two scale of the amplitudes of an n-qubit state inside the
+// operands: 2^min(max(n/2 - 2, 0), 12), so a normalised state's amplitudes
+// (at most 1) stay below 2^12 and typical ones (2^(-n/2)) near 1/4.
+float tc_state_scale(int n);
 
 // Plan a lowered op list for the tensor-core pass mode (complex64, n >= 12).
 bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err);

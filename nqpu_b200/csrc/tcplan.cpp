@@ -9,8 +9,8 @@
 // generalised from 2 to 5 qubits); at most kTcMaxUnitaries clusters per pass,
 // the ops of any further cluster go back, in circuit order, ahead of the ops
 // the pass left out.  Each cluster becomes one 32x32 unitary accumulated in
-// FP64 with the engine's per-op arithmetic, then its real embedding is split
-// into TF32 hi/lo parts for the tensor cores.
+// FP64 with the engine's per-op arithmetic, then the real embedding of 16 U is
+// split into FP16 hi/lo parts for the tensor cores.
 //
 // Layouts: for unitary j the planner also picks which tile bits are the
 // operand's row bits 0..4.  Those decide the shared-memory banks of the
@@ -36,30 +36,19 @@ namespace {
 
 int popc(uint64_t x) { return __builtin_popcountll(x); }
 
-uint32_t rn_tf32(float x) {
-  uint32_t b;
-  std::memcpy(&b, &x, 4);
-  return (b + 0x1000u) & 0xFFFFE000u;
-}
-float as_float(uint32_t b) {
-  float f;
-  std::memcpy(&f, &b, 4);
-  return f;
-}
-
 // Byte offsets of the tile bits in a layout (frow / fcol given).
 void layout_offsets(const int* frow, const int* fcol, uint32_t* boff) {
-  for (int i = 0; i < 7; ++i) boff[frow[i]] = tc_sw128_off<128>(1u << i, 0);
-  for (int i = 0; i < 5; ++i) boff[fcol[i]] = tc_sw128_off<128>(0, 2u << i);
+  for (int i = 0; i < 7; ++i) boff[frow[i]] = tc_sw128_off(1u << i, 0);
+  for (int i = 0; i < 5; ++i) boff[fcol[i]] = tc_sw128_off(0, 2u << i);  // complex column bit i = half 2 << i
 }
 
-// GF(2) rank of 4-bit vectors (bits above 3 ignored).
-int rank4(const uint32_t* v, int cnt) {
-  uint32_t basis[4] = {0, 0, 0, 0};
+// GF(2) rank of 5-bit vectors (bits above 4 ignored).
+int rank5(const uint32_t* v, int cnt) {
+  uint32_t basis[5] = {0, 0, 0, 0, 0};
   int r = 0;
   for (int i = 0; i < cnt; ++i) {
-    uint32_t x = v[i] & 15u;
-    for (int b = 3; b >= 0; --b) {
+    uint32_t x = v[i] & 31u;
+    for (int b = 4; b >= 0; --b) {
       if (!((x >> b) & 1u)) continue;
       if (!basis[b]) {
         basis[b] = x;
@@ -72,20 +61,25 @@ int rank4(const uint32_t* v, int cnt) {
   return r;
 }
 
-// Shared-memory wavefronts of one warp-wide store whose lanes run over the
-// tile bits lb[0..4], into a layout with byte offsets boff.  8-byte stores go
-// out a half warp (lane bits 0..3) at a time and are conflict-free when the
-// lanes' images in address bits 3..6 are independent; 16-byte stores go out a
-// quarter warp (lane bits 0..2) at a time and need address bits 4..6.  (The
-// kernel's ncu store-wavefront counts follow this rule.)
-int store_wavefronts(const int* lb, const uint32_t* boff, bool wide) {
-  uint32_t v[4];
-  if (wide) {
+// Shared-memory wavefronts of one warp-wide store of `width` bytes per lane
+// whose lanes run over the tile bits lb[0..4], into a layout with byte offsets
+// boff.  A 4-byte store is one wavefront when the lanes' images in address
+// bits 2..6 (the bank) are independent; 8-byte stores go out a half warp
+// (lane bits 0..3, address bits 3..6) and 16-byte stores a quarter warp (lane
+// bits 0..2, address bits 4..6) at a time.  (The kernel's ncu store-wavefront
+// counts follow this rule.)
+int store_wavefronts(const int* lb, const uint32_t* boff, int width) {
+  uint32_t v[5];
+  if (width == 16) {
     for (int i = 0; i < 3; ++i) v[i] = (boff[lb[i]] >> 4) & 7u;
-    return 4 << (3 - rank4(v, 3));
+    return 4 << (3 - rank5(v, 3));
   }
-  for (int i = 0; i < 4; ++i) v[i] = boff[lb[i]] >> 3;
-  return 2 << (4 - rank4(v, 4));
+  if (width == 8) {
+    for (int i = 0; i < 4; ++i) v[i] = (boff[lb[i]] >> 3) & 15u;
+    return 2 << (4 - rank5(v, 4));
+  }
+  for (int i = 0; i < 5; ++i) v[i] = (boff[lb[i]] >> 2) & 31u;
+  return 1 << (5 - rank5(v, 5));
 }
 
 // Layout choice of a pass: column order and row order of every unitary's
@@ -104,13 +98,16 @@ int layout_cost(const LayoutCfg& c, int m, const int* qt) {
   uint32_t boff[kTcMaxUnitaries][12];
   for (int j = 0; j < m; ++j) layout_offsets(c.frow[j], c.fcol[j], boff[j]);
   int cost = 0;
-  // loader: 16 warps x 4 steps, lanes over tile bits lt[0..4], hi and lo planes
-  if (c.fcol[0][0] == 0) cost += 64 * 2 * store_wavefronts(c.lt, boff[0], true);
-  else cost += 64 * 2 * 2 * store_wavefronts(c.lt, boff[0], false);
-  // epilogue: 16 warps x 8 columns (4 instructions of 16 bytes or 8 of 8)
+  // loader: 8 warps x 8 steps, lanes over tile bits lt[0..4], hi and lo
+  // planes; the two amplitudes of a 16-byte load are one 8-byte store when
+  // tile bit 0 is column bit 0 of unitary 0, else two 4-byte stores
+  if (c.fcol[0][0] == 0) cost += 64 * 2 * store_wavefronts(c.lt, boff[0], 8);
+  else cost += 64 * 2 * 2 * store_wavefronts(c.lt, boff[0], 4);
+  // epilogue: 8 warps x 16 columns, pairs of columns as 8-byte stores when
+  // both layouts share column bit 0
   for (int j = 0; j + 1 < m; ++j) {
     const bool pair = c.fcol[j][0] == c.fcol[j + 1][0];
-    cost += 16 * (pair ? 4 : 8) * 2 * store_wavefronts(c.frow[j], boff[j + 1], pair);
+    cost += 8 * (pair ? 8 : 16) * 2 * store_wavefronts(c.frow[j], boff[j + 1], pair ? 8 : 4);
   }
   // HBM: lanes over rows 0..4 of the last layout.  A 32-byte sector holds the
   // 4 amplitudes that differ in qubits 0 and 1 (tile bits 0 and 1), so a warp
@@ -214,10 +211,10 @@ void choose_layouts(TcPassRec& P) {
   };
   LayoutCfg best = cur;
   int bestc = descend(best);
-  // lower bound: conflict-free stores (the loader's 16-byte or 8-byte stores
-  // move the same 512 wavefronts per tile, as does each epilogue into a next
-  // operand) and fully used HBM sectors
-  const int bound = 512 * m;
+  // lower bound: conflict-free stores (the loader's stores move 256
+  // wavefronts per tile, as does each epilogue into a next operand) and fully
+  // used HBM sectors
+  const int bound = 256 * m;
   for (int restart = 0; restart < 40 && bestc > bound; ++restart) {
     LayoutCfg t = cur;
     for (int j = 0; j < m; ++j) {
@@ -239,8 +236,51 @@ void choose_layouts(TcPassRec& P) {
 
 }  // namespace
 
+uint16_t tc_half_bits(float x) {
+  uint32_t f;
+  std::memcpy(&f, &x, 4);
+  const uint32_t sign = (f >> 16) & 0x8000u;
+  const uint32_t absf = f & 0x7FFFFFFFu;
+  if (absf >= 0x7F800000u) return uint16_t(sign | 0x7C00u | (absf > 0x7F800000u ? 0x200u : 0u));  // inf / nan
+  if (absf >= 0x477FF000u) return uint16_t(sign | 0x7C00u);  // rounds past 65504: overflow to inf
+  if (absf < 0x38800000u) {
+    // subnormal half (|x| < 2^-14): value = m * 2^-24, round to nearest even
+    if (absf < 0x33000000u) return uint16_t(sign);  // below half of the smallest subnormal
+    const uint32_t e = absf >> 23;
+    const uint32_t mant = (absf & 0x7FFFFFu) | 0x800000u;
+    const uint32_t shift = 126u - e;  // 14 + (127 - e) - 1 - 10 + 24 - 23 ...: bits dropped
+    const uint32_t q = mant >> shift, rem = mant & ((1u << shift) - 1u), half = 1u << (shift - 1u);
+    const uint32_t r = q + ((rem > half || (rem == half && (q & 1u))) ? 1u : 0u);
+    return uint16_t(sign | r);
+  }
+  // normal: re-bias the exponent, round the mantissa to 10 bits (nearest even)
+  const uint32_t rem = absf & 0x1FFFu, base = (absf - 0x38000000u) >> 13;
+  const uint32_t r = base + ((rem > 0x1000u || (rem == 0x1000u && (base & 1u))) ? 1u : 0u);
+  return uint16_t(sign | r);
+}
+
+float tc_half_value(uint16_t h) {
+  const uint32_t sign = uint32_t(h & 0x8000u) << 16, e = (h >> 10) & 0x1Fu, mant = h & 0x3FFu;
+  uint32_t f;
+  if (e == 0) {
+    const float v = float(mant) * 5.9604644775390625e-8f;  // 2^-24
+    return (h & 0x8000u) ? -v : v;
+  }
+  if (e == 31) f = sign | 0x7F800000u | (mant << 13);
+  else f = sign | ((e + 112u) << 23) | (mant << 13);
+  float out;
+  std::memcpy(&out, &f, 4);
+  return out;
+}
+
+float tc_state_scale(int n) {
+  const int e = std::min(std::max(n / 2 - 2, 0), 12);
+  return float(1u << e);
+}
+
 bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err) {
   out->n = n;
+  out->state_scale = tc_state_scale(n);
   out->passes.clear();
   out->bmats.clear();
   out->unitaries.clear();
@@ -339,7 +379,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
   std::vector<size_t> first_u(np + 1, 0);
   for (size_t i = 0; i < np; ++i) first_u[i + 1] = first_u[i] + size_t(out->passes[i].m);
   out->unitaries.assign(first_u[np], {});
-  out->bmats.assign(first_u[np] * kTcBmatFloats, 0.0f);
+  out->bmats.assign(first_u[np] * kTcBmatHalves, uint16_t(0));
   auto finish_pass = [&](size_t pi) {
     TcPassRec& P = out->passes[pi];
     choose_layouts(P);
@@ -369,16 +409,16 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
         for (int idx : cluster_ops[ui]) fusion_apply_local(ops[size_t(idx)], q, col);
         for (int r = 0; r < 32; ++r) u[size_t(r * 32 + c)] = col[r];
       }
-      float* B = out->bmats.data() + ui * kTcBmatFloats;
+      uint16_t* B = out->bmats.data() + ui * kTcBmatHalves;
       for (int co = 0; co < 32; ++co)
         for (int ci = 0; ci < 32; ++ci) {
-          const cplx v = u[size_t(co * 32 + ci)];
+          const cplx v = double(kTcUScale) * u[size_t(co * 32 + ci)];
           const double e[2][2] = {{v.real(), -v.imag()}, {v.imag(), v.real()}};
           for (int a = 0; a < 2; ++a)
             for (int b = 0; b < 2; ++b) {
               const int nrow = 2 * co + a, k = 2 * ci + b;
-              const float hi = as_float(rn_tf32(float(e[a][b])));
-              const float lo = as_float(rn_tf32(float(e[a][b] - double(hi))));
+              const uint16_t hi = tc_half_bits(float(e[a][b]));
+              const uint16_t lo = tc_half_bits(float(e[a][b] - double(tc_half_value(hi))));
               B[nrow * 64 + k] = hi;
               B[(64 + nrow) * 64 + k] = lo;
             }
@@ -399,7 +439,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
   }
   out->stats.passes = out->passes.size();
   out->stats.ops = ops.size();
-  out->stats.upload_bytes = out->passes.size() * sizeof(TcPassRec) + out->bmats.size() * sizeof(float);
+  out->stats.upload_bytes = out->passes.size() * sizeof(TcPassRec) + out->bmats.size() * sizeof(uint16_t);
   return true;
 }
 

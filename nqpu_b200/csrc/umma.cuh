@@ -1,7 +1,7 @@
 // sm_100a tensor-core helpers shared by the fused-unitary kernel (fused.cu)
 // and the tensor-core pass kernel (tcpass.cu): TF32 rounding, shared-memory
-// operand descriptors (K-major, 128-byte swizzle), tcgen05.mma kind::tf32,
-// mbarriers with bounded polling.  Hand-written PTX; included by .cu files only.
+// operand descriptors (K-major, 128-byte swizzle), tcgen05.mma kind::tf32 and
+// kind::f16, tensor-memory loads, mbarriers with bounded polling.  Hand-written PTX; included by .cu files only.
 #pragma once
 #include <cstdint>
 
@@ -31,6 +31,24 @@ template <uint32_t M, uint32_t N>
 constexpr uint32_t umma_idesc_tf32() {
   static_assert(M == 128 && N % 16 == 0 && N >= 16 && N <= 256, "cta_group::1 shape");
   return (1u << 4) | (2u << 7) | (2u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// Instruction descriptor of kind::f16 with FP16 A and B: D fp32, both K-major, M x N.
+template <uint32_t M, uint32_t N>
+constexpr uint32_t umma_idesc_f16() {
+  static_assert(M == 128 && N % 16 == 0 && N >= 16 && N <= 256, "cta_group::1 shape");
+  return (1u << 4) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T with FP16 operands (K = 16), issued by one thread.
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread.
@@ -102,6 +120,12 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
 // Shared-memory stores through 32-bit shared-window addresses.
 __device__ __forceinline__ void sts_v2(uint32_t addr, float a, float b) {
   asm volatile("st.shared.v2.f32 [%0], {%1, %2};\n" ::"r"(addr), "f"(a), "f"(b) : "memory");
+}
+__device__ __forceinline__ void sts_b32(uint32_t addr, uint32_t a) {
+  asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(addr), "r"(a) : "memory");
+}
+__device__ __forceinline__ void sts_v2_b32(uint32_t addr, uint32_t a, uint32_t b) {
+  asm volatile("st.shared.v2.b32 [%0], {%1, %2};\n" ::"r"(addr), "r"(a), "r"(b) : "memory");
 }
 __device__ __forceinline__ void sts_v4(uint32_t addr, float a, float b, float c, float d) {
   asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");

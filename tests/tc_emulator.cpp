@@ -1,12 +1,13 @@
 // Test infrastructure: a CPU emulation of the tensor-core pass kernel
 // (nqpu_b200/csrc/tcpass.cu).  It executes the planner's pass records with the
 // kernel's index arithmetic — the loader's per-thread / per-step address and
-// operand-offset parts, the 128-byte-swizzled K-major operand images, the B
-// operand copy, the contraction D = A B^T over those images, the epilogue's
-// row / column offset tables into the next operand layout or HBM, and the
-// 16-byte pairing conditions — in FP64, optionally with the kernel's TF32
-// hi/lo split.  Every operand slot and every amplitude must be written exactly
-// once per tile, which checks that each layout is a bijection.
+// operand-offset parts, the 128-byte-swizzled K-major FP16 operand images, the
+// B operand copy, the contraction D = A B^T over those images, the epilogue's
+// row / column offset tables into the next operand layout or HBM, the state
+// and unitary scale factors, and the 8- and 16-byte pairing conditions — in
+// FP64, optionally with the kernel's FP16 hi/lo split.  Every operand slot and
+// every amplitude must be written exactly once per tile, which checks that
+// each layout is a bijection.
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -21,39 +22,35 @@ using namespace nqpu;
 
 namespace {
 
-float tf32(float x) {
-  uint32_t b;
-  std::memcpy(&b, &x, 4);
-  b = (b + 0x1000u) & 0xFFFFE000u;
-  float f;
-  std::memcpy(&f, &b, 4);
-  return f;
-}
+double half_round(double x) { return double(tc_half_value(tc_half_bits(float(x)))); }
 
+// One FP16 operand plane pair: 8192 half slots each, indexed by byte offset / 2.
 struct Operand {
-  std::vector<double> hi, lo;   // 8192 fp32 slots each, indexed by byte offset / 4
+  std::vector<double> hi, lo;
   std::vector<int> written;
   void clear() {
     hi.assign(8192, 0.0);
     lo.assign(8192, 0.0);
     written.assign(8192, 0);
   }
-  // store (re, im) at byte offset o (8-byte aligned) as the kernel's put2 does
+  // store the (re, im) half pair at byte offset o (4-byte aligned), as the
+  // kernel's split does: hi = half(x), lo = half(x - hi), x an fp32 value
   bool put(uint32_t o, double re, double im, bool split) {
-    if (o % 8 != 0 || o + 8 > 32768) return false;
-    const uint32_t s = o / 4;
+    if (o % 4 != 0 || o + 4 > 16384) return false;
+    const uint32_t s = o / 2;
     if (written[s] || written[s + 1]) return false;
     written[s] = written[s + 1] = 1;
-    if (split) {
-      const float hr = tf32(float(re)), hm = tf32(float(im));
-      hi[s] = hr;
-      hi[s + 1] = hm;
-      lo[s] = tf32(float(re) - hr);
-      lo[s + 1] = tf32(float(im) - hm);
-    } else {
-      hi[s] = re;
-      hi[s + 1] = im;
-      lo[s] = lo[s + 1] = 0.0;
+    const double v[2] = {re, im};
+    for (int i = 0; i < 2; ++i) {
+      if (split) {
+        const float x = float(v[i]);
+        const double h = half_round(x);
+        hi[s + i] = h;
+        lo[s + i] = half_round(double(x) - h);
+      } else {
+        hi[s + i] = v[i];
+        lo[s + i] = 0.0;
+      }
     }
     return true;
   }
@@ -61,9 +58,11 @@ struct Operand {
 
 }  // namespace
 
+extern "C" uint16_t emu_half_bits(float x) { return tc_half_bits(x); }
+
 // Returns the number of passes (>= 0) or a negative error code:
 // -1 plan failed, -2 operand slot written twice / misaligned, -3 amplitude
-// written twice or not at all, -4 a 16-byte pairing condition does not hold,
+// written twice or not at all, -4 a pairing condition does not hold,
 // -5 the loader's bit map is not a permutation with tile bits 1..3 first.
 extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, int split, int64_t* stats) {
   std::vector<GateRec> gates(static_cast<size_t>(ngates));
@@ -80,46 +79,45 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
   std::string err;
   if (!build_tc_plan(lower_circuit(gates), n, &plan, &err)) return -1;
   const size_t dim = size_t(1) << n;
+  const double sc = plan.state_scale, uinv = 1.0 / double(kTcUScale);
   std::vector<double> st(state, state + 2 * dim);
   const uint64_t n_tiles = 1ull << (n - kTcTileBits);
   size_t boff_base = 0;
   int64_t unitaries = 0;
+  const int nthr = 1 << kTcLoadThreadBits, nstep = 1 << kTcLoadStepBits;
   for (const TcPassRec& P : plan.passes) {
     const int m = P.m;
     unitaries += m;
-    // B operands as the kernel's shared-memory images
-    // (FP64 mode: the exact real embedding of the planner's FP64 unitary in
-    // rows 0..63 and zeros in rows 64..127, so the algebra is checked exactly)
+    // B operands as the kernel's shared-memory images (FP64 mode: the exact
+    // real embedding of 16 U in rows 0..63 and zeros in rows 64..127, so the
+    // algebra is checked exactly)
     std::vector<std::vector<double>> bimg(static_cast<size_t>(m), std::vector<double>(8192, 0.0));
     for (int j = 0; j < m; ++j) {
-      const float* B = plan.bmats.data() + boff_base + size_t(j) * kTcBmatFloats;
+      const uint16_t* B = plan.bmats.data() + boff_base + size_t(j) * kTcBmatHalves;
       const std::vector<cplx>& U = plan.unitaries[size_t(unitaries - m + j)];
       for (uint32_t nrow = 0; nrow < 128; ++nrow)
         for (uint32_t k = 0; k < 64; ++k) {
-          double v = B[nrow * 64 + k];
+          double v = tc_half_value(B[nrow * 64 + k]);
           if (!split) {
-            const cplx u = nrow < 64 ? U[(nrow / 2) * 32 + k / 2] : cplx(0, 0);
+            const cplx u = nrow < 64 ? double(kTcUScale) * U[(nrow / 2) * 32 + k / 2] : cplx(0, 0);
             const double e[2][2] = {{u.real(), -u.imag()}, {u.imag(), u.real()}};
             v = nrow < 64 ? e[nrow & 1][k & 1] : 0.0;
           }
-          bimg[size_t(j)][tc_sw128_off<128>(nrow, k) / 4] = v;
+          bimg[size_t(j)][tc_sw128_off(nrow, k) / 2] = v;
         }
     }
-    boff_base += size_t(m) * kTcBmatFloats;
-    // loader tables (kernel: T->sol / T->sgl and the per-thread pol / pgl)
-    // (512 loading threads, 4 steps: thread bit b -> tile bit lt[b], step bit
-    // s -> tile bit lt[9 + s], tile bit 0 = the pair inside a 16-byte load)
-    uint32_t sol[4];
-    uint64_t sgl[4];
-    for (int i = 0; i < 4; ++i) {
-      sol[i] = 0;
-      sgl[i] = 0;
-      for (int s = 0; s < 2; ++s)
+    boff_base += size_t(m) * kTcBmatHalves;
+    // loader tables (kernel: T->sol / T->sgl and the per-thread pol / pgl):
+    // thread bit b -> tile bit lt[b], step bit s -> tile bit lt[kTcLoadThreadBits + s],
+    // tile bit 0 = the pair inside a 16-byte load
+    std::vector<uint32_t> sol(size_t(nstep), 0);
+    std::vector<uint64_t> sgl(size_t(nstep), 0);
+    for (int i = 0; i < nstep; ++i)
+      for (int s = 0; s < kTcLoadStepBits; ++s)
         if ((i >> s) & 1) {
-          sol[i] ^= P.u[0].boff[P.lt[9 + s]];
-          sgl[i] |= 1ull << P.qt[P.lt[9 + s]];
+          sol[size_t(i)] ^= P.u[0].boff[P.lt[kTcLoadThreadBits + s]];
+          sgl[size_t(i)] |= 1ull << P.qt[P.lt[kTcLoadThreadBits + s]];
         }
-    }
     {
       uint32_t seen = 1u;  // the loader map must be a permutation of tile bits 1..11
       for (int b = 0; b < 11; ++b) {
@@ -129,7 +127,7 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
       if (P.lt[0] != 1 || P.lt[1] != 2 || P.lt[2] != 3) return -5;
     }
     const uint32_t boff_h = P.u[0].boff[0];
-    const bool load16 = boff_h == 8u;
+    const bool load_pair = boff_h == 4u;  // tile bit 0 is column bit 0 of unitary 0
     const bool store16 = P.qt[P.u[m - 1].fcol[0]] == 0;
     std::vector<int> amp_written(dim, 0);
     for (uint64_t tile = 0; tile < n_tiles; ++tile) {
@@ -138,35 +136,34 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
         if ((tile >> j) & 1ull) tb |= 1ull << P.qout[j];
       Operand A;
       A.clear();
-      for (uint32_t gt = 0; gt < 512; ++gt) {
+      for (int gt = 0; gt < nthr; ++gt) {
         uint32_t pol = 0;
         uint64_t pgl = 0;
-        for (int b = 0; b < 9; ++b)
+        for (int b = 0; b < kTcLoadThreadBits; ++b)
           if ((gt >> b) & 1) {
             pol ^= P.u[0].boff[P.lt[b]];
             pgl |= 1ull << P.qt[P.lt[b]];
           }
-        for (int i = 0; i < 4; ++i) {
-          const uint64_t a = tb + pgl + sgl[i];  // even: the float4 of amplitudes a, a + 1
+        for (int i = 0; i < nstep; ++i) {
+          const uint64_t a = tb + pgl + sgl[size_t(i)];  // even: the 16-byte load of amplitudes a, a + 1
           if (a & 1ull) return -3;
-          const uint32_t o = pol ^ sol[i];
-          if (load16 && (o & 15u)) return -4;
-          if (!A.put(o, st[2 * a], st[2 * a + 1], split != 0)) return -2;
-          if (!A.put(o ^ boff_h, st[2 * a + 2], st[2 * a + 3], split != 0)) return -2;
-          if (load16 && (o ^ boff_h) != o + 8) return -4;
+          const uint32_t o = pol ^ sol[size_t(i)];
+          if (load_pair && ((o & 7u) || (o ^ boff_h) != o + 4)) return -4;
+          if (!A.put(o, sc * st[2 * a], sc * st[2 * a + 1], split != 0)) return -2;
+          if (!A.put(o ^ boff_h, sc * st[2 * a + 2], sc * st[2 * a + 3], split != 0)) return -2;
         }
       }
       for (int s = 0; s < 8192; ++s)
         if (!A.written[size_t(s)]) return -2;
       for (int j = 0; j < m; ++j) {
         const std::vector<double>& Bi = bimg[size_t(j)];
-        // D[r][0:128] = A_hi [R_hi; R_lo]^T ; D[r][0:64] += A_lo R_hi^T
+        // D[r][0:128] = A_hi [B_hi; B_lo]^T ; D[r][0:64] += A_lo B_hi^T
         std::vector<double> D(128 * 128, 0.0);
         for (uint32_t r = 0; r < 128; ++r)
           for (uint32_t nn = 0; nn < 128; ++nn) {
             double acc = 0.0;
             for (uint32_t k = 0; k < 64; ++k) {
-              const uint32_t ao = tc_sw128_off<128>(r, k) / 4, bo = tc_sw128_off<128>(nn, k) / 4;
+              const uint32_t ao = tc_sw128_off(r, k) / 2, bo = tc_sw128_off(nn, k) / 2;
               acc += A.hi[ao] * Bi[bo];
               if (nn < 64) acc += A.lo[ao] * Bi[bo];
             }
@@ -183,17 +180,17 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
               if (!last) ptn ^= P.u[j + 1].boff[P.u[j].frow[i]];
               else pg |= 1ull << P.qt[P.u[j].frow[i]];
             }
-          const bool pair16 = !last && P.u[j + 1].boff[P.u[j].fcol[0]] == 8u;
+          const bool pair = !last && P.u[j + 1].boff[P.u[j].fcol[0]] == 4u;
           for (uint32_t c = 0; c < 32; ++c) {
-            double re = D[r * 128 + 2 * c] + D[r * 128 + 64 + 2 * c];
-            double im = D[r * 128 + 2 * c + 1] + D[r * 128 + 64 + 2 * c + 1];
+            double re = (D[r * 128 + 2 * c] + D[r * 128 + 64 + 2 * c]) * uinv;
+            double im = (D[r * 128 + 2 * c + 1] + D[r * 128 + 64 + 2 * c + 1]) * uinv;
             if (split) {
               re = double(float(re));
               im = double(float(im));
             }
             if (!last) {
               const uint32_t o = ptn ^ P.u[j].xnext[c];
-              if (pair16 && (c & 1u) == 0 && ((o & 15u) || (ptn ^ P.u[j].xnext[c + 1]) != o + 8)) return -4;
+              if (pair && (c & 1u) == 0 && ((o & 7u) || (ptn ^ P.u[j].xnext[c + 1]) != o + 4)) return -4;
               if (!N.put(o, re, im, split != 0)) return -2;
             } else {
               const uint64_t a = tb + pg + P.u[j].gcol[c];
@@ -201,8 +198,8 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
               if (store16 && (c & 1u) == 1 && P.u[j].gcol[c] != P.u[j].gcol[c - 1] + 1) return -4;
               if (a >= dim || amp_written[a]) return -3;
               amp_written[a] = 1;
-              st[2 * a] = re;
-              st[2 * a + 1] = im;
+              st[2 * a] = re / sc;
+              st[2 * a + 1] = im / sc;
             }
           }
         }

@@ -1,5 +1,5 @@
 """GPU parity of the tensor-core pass mode (NQPU_MODE_TENSOR, tcpass.cu):
-up to two fused 5-qubit unitaries per HBM pass, split-TF32 tcgen05 GEMMs on a
+up to three fused 5-qubit unitaries per HBM pass, split-FP16 tcgen05 GEMMs on a
 shared-memory tile, complex64 states of 12 or more qubits.
 
 Tolerance (complex64 against the FP64 oracle, as every complex64 test):
@@ -127,7 +127,7 @@ def test_agrees_with_tiled_engine():
     c.execute(b, "tiled")
     assert 1 - a.fidelity(b) <= TOL
     st = c.plan_stats(n, "c64", "tensor")
-    assert st["passes"] >= 1 and st["stages"] <= 2 * st["passes"]
+    assert st["passes"] >= 1 and st["stages"] <= 3 * st["passes"]  # at most three unitaries per pass
     a.close()
     b.close()
 
