@@ -4,12 +4,15 @@
 Default workload (one step = one full circuit run):
   30-qubit random brickwork circuit, depth 40 (1200 U3 + 580 CNOT = 1780 gates),
   complex64 state (8 GiB, larger than L2 -> no flush needed), |0..0> reset,
-  every gate applied unfused by the tiled pass engine, then all <Z_i> (FP64).
+  the circuit run by the tensor pass engine (per HBM pass up to three fused
+  5-qubit unitaries as split-FP16 tcgen05 GEMMs), then all <Z_i> (FP64).
   metric = gates/s (original gates per second, whole job over all ranks).
 
 Also reported (one untimed run each): the complex128 run of the same circuit
-and 1-F / max|d<Z_i>| of complex64 against it; the plain per-gate path (one
-kernel launch per gate) and its algorithmic HBM GB/s.
+and 1-F / max|d<Z_i>| of complex64 against it and against the complex128
+per-gate path; the unfused tiled engine (every gate applied on its own to a
+shared-memory tile) and the plain per-gate path (one kernel launch per gate)
+with their times and algorithmic HBM GB/s.
 
   python bench.py [--gpus N --steps K --warmup W]     engine arm
   python bench.py --impl reference                   CPU reference arm (oracle port)
@@ -166,7 +169,7 @@ def run_reference(args):
     value = cnt / el
     cores = O.max_threads()
     line = {
-        "impl": "reference", "metric": f"gates/s ({n}q {'complex64' if f32 else 'complex128'} brickwork, unfused)",
+        "impl": "reference", "metric": f"gates/s ({n}q {'complex64' if f32 else 'complex128'} brickwork)",
         "value": value,
         "unit": "gates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * el / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -191,6 +194,30 @@ DRAM_BYTES_PER_AMP = {
 }
 
 
+MODE_DESCRIPTIONS = {
+    "tensor": "per HBM pass, up to 3 fused 5-qubit unitaries (32x32 complex, every original gate "
+              "folded in) as tcgen05 GEMMs on split-FP16 operands with FP32 accumulation",
+    "tiled": "per HBM pass, every gate applied on its own (unfused) to a 2^12-amplitude shared-memory tile, "
+             "SIMT FP32/FP64",
+    "pergate": "one kernel per gate over the whole state",
+    "fused": "one 5-qubit fused unitary per launch, split-TF32 tcgen05 GEMM",
+}
+
+
+def tc_pass_flops(unitaries, n):
+    """Tensor-core FLOPs of the tensor pass mode: every fused unitary runs, on
+    each 2^12-amplitude tile, A_hi [B_hi; B_lo]^T (128 x 128 x 64) and
+    A_lo B_hi^T (128 x 64 x 64)."""
+    return unitaries * (1 << (n - 12)) * 2 * 128 * 64 * (128 + 64)
+
+
+def tensor_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["bf16_tflops"])
+    return 1590.0
+
+
 def traffic_per_launch(kernel, n):
     b = DRAM_BYTES_PER_AMP.get(kernel)
     return None if b is None else b * (1 << n)
@@ -213,6 +240,8 @@ def run_engine(args):
     lib = _lib.load()
 
     n, depth = args.qubits, args.depth
+    if args.mode == "auto":
+        args.mode = "tensor" if args.dtype == "c64" and n >= 12 else "tiled"
     if args.tile_ctas:
         _lib.check(lib.nqpu_tile_config_set(1 if args.dtype == "c64" else 0, args.tile_ctas), "tile_config")
     if args.circuit == "qft":
@@ -284,16 +313,24 @@ def run_engine(args):
                 "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
                 "launches_per_step": stats["passes"], "avg_launch_ms": avg_launch_ms,
                 "pass_time_share": (sum(launch_ms) / el_ms) if el_ms else None}
-    # the tiled pass is bound by FP32 issue, not HBM: its arithmetic rate against
-    # the FP32 peak (148 SMs x 128 lanes x 2 flops per cycle at the sampled clock)
-    from nqpu_b200.circuits import algorithmic_flops
     mhz = (clk or {}).get("sm_mhz") or 1965.0
-    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
     pass_s = sum(launch_ms) / 1000.0 if launch_ms else float("nan")
-    fl = algorithmic_flops(gates, n) * args.steps
-    roofline["fp32"] = {"achieved_tflops": fl / pass_s / 1e12, "peak_tflops": fp32_peak,
-                        "frac": fl / pass_s / 1e12 / fp32_peak, "flops_per_step": fl // args.steps,
-                        "peak_kind": "nominal at the sampled SM clock"}
+    if args.mode == "tensor":
+        # tensor-pipe work of the pass kernel: per tile (2^12 amplitudes) and
+        # fused unitary, a 128 x 128 x 64 and a 128 x 64 x 64 FP16 GEMM
+        fl = tc_pass_flops(stats["stages"], n) * args.steps
+        roofline["tensor"] = {"achieved_tflops": fl / pass_s / 1e12, "peak_tflops": tensor_peak(),
+                              "frac": fl / pass_s / 1e12 / tensor_peak(), "flops_per_step": fl // args.steps,
+                              "peak_kind": "measured dense bf16 (cuBLAS burst); FP16 runs at the same rate"}
+    elif args.mode == "tiled":
+        # the tiled pass is bound by FP32 issue, not HBM: its arithmetic rate against
+        # the FP32 peak (148 SMs x 128 lanes x 2 flops per cycle at the sampled clock)
+        from nqpu_b200.circuits import algorithmic_flops
+        fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        fl = algorithmic_flops(gates, n) * args.steps
+        roofline["fp32"] = {"achieved_tflops": fl / pass_s / 1e12, "peak_tflops": fp32_peak,
+                            "frac": fl / pass_s / 1e12 / fp32_peak, "flops_per_step": fl // args.steps,
+                            "peak_kind": "nominal at the sampled SM clock"}
     launches_per_step = stats["passes"] + 1 + 2  # passes + reset + zsums (2 kernels)
 
     extra = {}
@@ -320,10 +357,10 @@ def run_engine(args):
             zpg = svpg.expectation_z_all()
             extra["accuracy_vs_pergate"] = {
                 "reference": "complex128 per-gate path (one kernel per gate, no tiled plan)",
-                "tiled_c64": {"one_minus_F": 1.0 - sv.fidelity(svpg),
-                              "max_abs_dZ": float(np.abs(z_c64 - zpg).max())},
-                "tiled_c128": {"one_minus_F": 1.0 - sv128.fidelity(svpg),
-                               "max_abs_dZ": float(np.abs(z128 - zpg).max())},
+                f"{args.mode}_c64": {"one_minus_F": 1.0 - sv.fidelity(svpg),
+                                     "max_abs_dZ": float(np.abs(z_c64 - zpg).max())},
+                f"{mode128}_c128": {"one_minus_F": 1.0 - sv128.fidelity(svpg),
+                                    "max_abs_dZ": float(np.abs(z128 - zpg).max())},
                 "tolerance": {"c64": 1e-5, "c128": 1e-12}}
             svpg.close()
             sv128.close()
@@ -345,6 +382,22 @@ def run_engine(args):
             "cnot_GBps": S / (np.mean(cx_ms) / 1000) / 1e9 if cx_ms else None,
             "frac_of_peak": algorithmic_bytes(gates, n, amp_bytes) / (tot_ms / 1000) / 1e9 / peak,
         }
+        if args.mode != "tiled":
+            # the unfused tiled engine on the same circuit: every gate applied
+            # on its own to the shared-memory tile (SIMT FP32), several per pass
+            tl_ms = (C.c_float * maxl)()
+            tcnt = C.c_uint32()
+            _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
+            _lib.check(lib.nqpu_circuit_execute_ex(circ.h_, sv.h_, MODES["tiled"]), "execute")  # warm
+            _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
+            _lib.check(lib.nqpu_circuit_profile(circ.h_, sv.h_, MODES["tiled"], tl_ms, maxl, C.byref(tcnt)),
+                       "profile")
+            tms = [tl_ms[i] for i in range(tcnt.value)]
+            extra["tiled_path"] = {
+                "gates_per_s": G / (sum(tms) / 1000), "seconds": sum(tms) / 1000, "passes": len(tms),
+                "kernel": "k_tile_pass", "avg_launch_ms": float(np.mean(tms)),
+                "frac_of_peak": 2 * S / (np.mean(tms) / 1000) / 1e9 / peak,
+                "timing": "CUDA events around each pass launch, one run after a warm-up run"}
 
     # e2e: host gate list -> circuit handle -> execute (plan build + H2D) -> <Z_i> D2H
     e2e = None
@@ -373,15 +426,16 @@ def run_engine(args):
 
     if rank == 0:
         line = {
-            "metric": (f"gates/s ({n}q {'complex64' if args.dtype == 'c64' else 'complex128'} brickwork, unfused)"
+            "metric": (f"gates/s ({n}q {'complex64' if args.dtype == 'c64' else 'complex128'} brickwork)"
                        if args.circuit == "brickwork"
-                       else f"gates/s ({n}q QFT, unfused)"), "value": value, "unit": "gates/s",
+                       else f"gates/s ({n}q QFT)"), "value": value, "unit": "gates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
             "config": {"workload": (f"brickwork {n}q depth {depth}" if args.circuit == "brickwork" else f"QFT {n}q")
                                    + f" {'complex64' if args.dtype == 'c64' else 'complex128'}",
                        "gates": G, "seed": args.seed, "engine_mode": args.mode,
+                       "engine": MODE_DESCRIPTIONS[args.mode],
                        "plan": {"passes": stats["passes"], "stages": stats["stages"]},
                        "tile_ctas_per_sm": int(lib.nqpu_tile_config_get(1 if args.dtype == "c64" else 0)),
                        "l2": f"state {S / 2**30:.2f} GiB vs 126 MB L2; no flush", "parallelism": f"replicas{world}"},
@@ -699,15 +753,23 @@ def run_batch(args):
     if not args.quick:
         t = time.perf_counter()
         cs = [Circuit.from_arrays(n, *a) for n, a, _, _ in arrs]
+        t_circ = time.perf_counter()
         b2 = Batch()
         b2.config(**cfg)
         for c, (n, g, J, h) in zip(cs, items):
             b2.add_ising(c, J, h)
+        t_add = time.perf_counter()
+        b2.prepare()
+        t_prep = time.perf_counter()
         r2 = b2.run()
-        et = time.perf_counter() - t
+        t_run = time.perf_counter()
+        et = t_run - t
         assert np.array_equal(r2, res)
         e2e = {"value": count / et, "unit": "circuits/s", "h2d_bytes_per_step": int(st["upload_bytes"]),
                "d2h_bytes_per_step": 8 * count, "seconds_per_step": et,
+               "phases_s": {"circuits": t_circ - t, "batch_add": t_add - t_circ, "prepare": t_prep - t_add,
+                            "run": t_run - t_prep},
+               "frac_of_device_rate": (count / et) / value,
                "timing": "host wall clock: Circuit handles from gate arrays (Circuit.from_arrays), batch add, "
                          "prepare (plans on host threads, uploads, graph capture), one replay, results on the host"}
         b2.close()
@@ -921,7 +983,8 @@ def main():
     ap.add_argument("--circuit", default="brickwork", choices=["brickwork", "qft"],
                     help="plain form circuit: random brickwork (headline) or the QFT")
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
-    ap.add_argument("--mode", default="tiled", choices=["tiled", "pergate", "fused", "tensor"])
+    ap.add_argument("--mode", default="auto", choices=["auto", "tiled", "pergate", "fused", "tensor"],
+                    help="engine mode of the plain form; auto = tensor for complex64 (n >= 12), else tiled")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--tile-ctas", type=int, default=0, help="tiled kernel CTAs per SM (1 or 2; 0 = library default)")
     ap.add_argument("--e2e-steps", type=int, default=2)

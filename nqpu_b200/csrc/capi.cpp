@@ -596,29 +596,41 @@ extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t
   if (count == 0) return NQPU_OK;
   if (!codes || !qubits || !params) return NQPU_NULL_POINTER;
   CircuitImpl* c = Cc(circuit);
-  std::vector<GateRec> add;
+  // the records are written in place after the existing gates and dropped
+  // again when any of them is rejected (the circuit is then unchanged)
+  const size_t base = c->gates.size();
   try {
-    add.reserve(count);
+    c->gates.resize(base + size_t(count));
   } catch (...) {
     return NQPU_ALLOCATION_FAILED;
   }
   // index arithmetic in size_t: 16 * count overflows 32 bits above 2^28 gates
   for (size_t i = 0; i < size_t(count); ++i) {
-    if (codes[i] >= uint32_t(G_COUNT)) return NQPU_INVALID_PARAMETER;
-    GateRec g = mk(uint8_t(codes[i]), qubits[3 * i], qubits[3 * i + 1], qubits[3 * i + 2], params[4 * i],
-                   params[4 * i + 1], params[4 * i + 2], params[4 * i + 3]);
-    // unused qubit slots are ignored
-    for (int k = g.nq; k < 3; ++k) g.q[k] = 0;
-    if (g.code == G_CUSTOM1 || g.code == G_CUSTOM2_FFI || g.code == G_U2_LO) {
-      if (!matrices) return NQPU_NULL_POINTER;
-      const int nm = g.code == G_CUSTOM1 ? 4 : 16;
-      for (int k = 0; k < nm; ++k) g.m[k] = cplx(matrices[16 * i + k].re, matrices[16 * i + k].im);
+    NqpuError e = NQPU_OK;
+    GateRec& g = c->gates[base + i];
+    if (codes[i] >= uint32_t(G_COUNT)) {
+      e = NQPU_INVALID_PARAMETER;
+    } else {
+      g.code = uint8_t(codes[i]);
+      g.nq = uint8_t(gate_arity(g.code));
+      for (int k = 0; k < 3; ++k) g.q[k] = k < g.nq ? qubits[3 * i + size_t(k)] : 0;  // unused slots ignored
+      for (int k = 0; k < 4; ++k) g.p[k] = params[4 * i + size_t(k)];
+      if (g.code == G_CUSTOM1 || g.code == G_CUSTOM2_FFI || g.code == G_U2_LO) {
+        if (!matrices) {
+          e = NQPU_NULL_POINTER;
+        } else {
+          const int nm = g.code == G_CUSTOM1 ? 4 : 16;
+          for (int k = 0; k < nm; ++k)
+            g.m[k] = cplx(matrices[16 * i + size_t(k)].re, matrices[16 * i + size_t(k)].im);
+        }
+      }
+      if (e == NQPU_OK) e = check_rec(c, g);
     }
-    const NqpuError e = check_rec(c, g);
-    if (e != NQPU_OK) return e;
-    add.push_back(g);
+    if (e != NQPU_OK) {
+      c->gates.resize(base);
+      return e;
+    }
   }
-  c->gates.insert(c->gates.end(), add.begin(), add.end());
   c->version++;
   return NQPU_OK;
 }

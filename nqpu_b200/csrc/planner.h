@@ -1,6 +1,8 @@
 // Host-side circuit representation, gate lowering and pass planning.
 #pragma once
+#include <array>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 #include "sv_types.h"
@@ -22,12 +24,30 @@ enum GateCode : uint8_t {
 };
 inline bool gate_is_mid(uint8_t code) { return code == G_MEASURE || code == G_RESET; }
 
+// The matrix of a custom gate (CUSTOM1: 2x2 in entries 0..3; CUSTOM2_FFI and
+// U2_LO: 4x4), held out of line and shared by copies of the record until one
+// of them writes (copy on write).  Records of the named gates carry none: a
+// null pointer that reads as zeros, so a record stays 64 bytes and circuits of
+// millions of gates copy and lower cheaply.
+class GateMatrix {
+ public:
+  cplx operator[](int i) const { return p_ ? (*p_)[size_t(i)] : cplx(0.0, 0.0); }
+  cplx& operator[](int i) {
+    if (!p_) p_ = std::make_shared<std::array<cplx, 16>>();
+    else if (p_.use_count() > 1) p_ = std::make_shared<std::array<cplx, 16>>(*p_);
+    return (*p_)[size_t(i)];
+  }
+
+ private:
+  std::shared_ptr<std::array<cplx, 16>> p_;
+};
+
 struct GateRec {
   uint8_t code = G_H;
   uint8_t nq = 1;
   int32_t q[3] = {0, 0, 0};
   double p[4] = {0, 0, 0, 0};
-  cplx m[16];  // custom matrices
+  GateMatrix m;  // custom matrices
 };
 
 int gate_arity(uint8_t code);

@@ -240,13 +240,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint64_t tb = tile_base_of(tile);
     // ---- load, scale, split into unitary 0's operand ----
     {
-      // pull this engine's next tile into L2 first (no registers held), so its
-      // loads will meet L2 rather than DRAM latency
-      if (tile + stride < n_tiles) {
-        const float4* nsrc = reinterpret_cast<const float4*>(amp) + ((tile_base_of(tile + stride) + pgl) >> 1);
-#pragma unroll
-        for (int i = 0; i < kTcLoadSteps; ++i) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(nsrc + (T->sgl[i] >> 1)));
-      }
       float4 v[kTcLoadSteps];
       const float4* src = reinterpret_cast<const float4*>(amp) + ((tb + pgl) >> 1);
 #pragma unroll
