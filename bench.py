@@ -240,8 +240,6 @@ def run_engine(args):
     lib = _lib.load()
 
     n, depth = args.qubits, args.depth
-    if args.mode == "auto":
-        args.mode = "tensor" if args.dtype == "c64" and n >= 12 else "tiled"
     if args.tile_ctas:
         _lib.check(lib.nqpu_tile_config_set(1 if args.dtype == "c64" else 0, args.tile_ctas), "tile_config")
     if args.circuit == "qft":
@@ -253,6 +251,12 @@ def run_engine(args):
     amp_bytes = 8 if args.dtype == "c64" else 16
     S = (1 << n) * amp_bytes
     circ = Circuit(n, gates)
+    if args.mode == "auto":
+        # the engine's own choice (NQPU_MODE_AUTO), timed as the mode it picks
+        am = C.c_int(-1)
+        _lib.check(lib.nqpu_circuit_auto_mode(circ.h_, n, 1 if args.dtype == "c64" else 0, C.byref(am)), "auto_mode")
+        args.mode = {v: k for k, v in MODES.items()}[am.value]
+        args.auto = True
     stats = circ.plan_stats(n, args.dtype, args.mode)
     sv = StateVector(n, args.dtype)
     stream = torch.cuda.ExternalStream(lib.nqpu_state_cuda_stream(sv.h_), device=dev)
@@ -409,14 +413,15 @@ def run_engine(args):
             t0 = time.perf_counter()
             c2 = Circuit(n, gates)
             _lib.check(lib.nqpu_state_reset(sv.h_), "reset")
-            _lib.check(lib.nqpu_circuit_execute_ex(c2.h_, sv.h_, MODES[args.mode]), "execute")
+            e2e_mode = MODES["auto"] if getattr(args, "auto", False) else MODES[args.mode]
+            _lib.check(lib.nqpu_circuit_execute_ex(c2.h_, sv.h_, e2e_mode), "execute")
             _lib.check(lib.nqpu_expectation_z_all(sv.h_, zptr, n), "zall")
             t_e2e.append(time.perf_counter() - t0)
             c2.close()
         et = replicas.max_over_ranks(float(np.mean(t_e2e)), device=dev)
         e2e = {"value": G * world / et, "unit": "gates/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 8 * n, "seconds_per_step": et,
-               "timing": "host wall clock around create+execute+reduce (includes plan build)"}
+               "timing": "host wall clock around create+execute+reduce (includes the mode choice and plan build)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.quick and not args.no_cpu:
@@ -435,6 +440,7 @@ def run_engine(args):
             "config": {"workload": (f"brickwork {n}q depth {depth}" if args.circuit == "brickwork" else f"QFT {n}q")
                                    + f" {'complex64' if args.dtype == 'c64' else 'complex128'}",
                        "gates": G, "seed": args.seed, "engine_mode": args.mode,
+                       "engine_mode_chosen_by": "NQPU_MODE_AUTO" if getattr(args, "auto", False) else "--mode",
                        "engine": MODE_DESCRIPTIONS[args.mode],
                        "plan": {"passes": stats["passes"], "stages": stats["stages"]},
                        "tile_ctas_per_sm": int(lib.nqpu_tile_config_get(1 if args.dtype == "c64" else 0)),
@@ -984,7 +990,7 @@ def main():
                     help="plain form circuit: random brickwork (headline) or the QFT")
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
     ap.add_argument("--mode", default="auto", choices=["auto", "tiled", "pergate", "fused", "tensor"],
-                    help="engine mode of the plain form; auto = tensor for complex64 (n >= 12), else tiled")
+                    help="engine mode of the plain form; auto = the engine's NQPU_MODE_AUTO choice")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--tile-ctas", type=int, default=0, help="tiled kernel CTAs per SM (1 or 2; 0 = library default)")
     ap.add_argument("--e2e-steps", type=int, default=2)

@@ -148,8 +148,10 @@ typedef enum {
     NQPU_MODE_TILED   = 0,  /* multi-gate smem/register tiled passes (default)       */
     NQPU_MODE_PERGATE = 1,  /* one full-state kernel launch per gate (plain per-gate) */
     NQPU_MODE_FUSED   = 2,  /* <=5-qubit fusion, split-TF32 tcgen05 contractions      */
-    NQPU_MODE_TENSOR  = 3   /* complex64, n >= 12: up to 2 fused 5-qubit unitaries per
-                               HBM pass, split-TF32 tcgen05 GEMMs on a shared-memory tile */
+    NQPU_MODE_TENSOR  = 3,  /* complex64, n >= 12: up to 3 fused 5-qubit unitaries per
+                               HBM pass, split-FP16 tcgen05 GEMMs on a shared-memory tile */
+    NQPU_MODE_AUTO    = 4   /* per gate run between mid-circuit measurements: the tensor
+                               mode when its modelled device time is lower, else tiled */
 } NqpuMode;
 
 /* Like nqpu_state_create with a dtype; 1 <= n <= 34 (HBM-bounded). */
@@ -308,10 +310,16 @@ NqpuError    nqpu_tile_config_set(NqpuDtype dtype, uint32_t ctas_per_sm);
 uint32_t     nqpu_tile_config_get(NqpuDtype dtype);
 /* Plan statistics of the last execution of `circuit` in `mode` on an n-qubit state:
  * out[0] = HBM passes (kernel launches over the full state), out[1] = lowered ops,
- * out[2] = register stages (tiled) or fused unitaries (fused), out[3] (when
- * len >= 4) = bytes of plan tables uploaded host->device per plan build.  len >= 3. */
+ * out[2] = register stages (tiled) or fused unitaries (fused, tensor), out[3]
+ * (when len >= 4) = bytes of plan tables uploaded host->device per plan build.
+ * len >= 3.  For NQPU_MODE_AUTO: the statistics of the modes it picks. */
 NqpuError    nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_t num_qubits,
                                      NqpuDtype dtype, NqpuMode mode, uint64_t* out, uint32_t len);
+/* The mode NQPU_MODE_AUTO runs the circuit's first gate run (up to its first
+ * mid-circuit measurement or reset) in on an n-qubit state of `dtype`:
+ * NQPU_MODE_TILED or NQPU_MODE_TENSOR (complex64, n >= 12 only). */
+NqpuError    nqpu_circuit_auto_mode(const NqpuCircuit* circuit, uint32_t num_qubits, NqpuDtype dtype,
+                                    NqpuMode* out);
 
 /* OpenQASM 2.0 (circuits/formats/qasm.rs:65 parse_qasm, :265 execute_qasm,
  * :363 export): qreg/creg declarations, the qelib1.inc gate set, parameter

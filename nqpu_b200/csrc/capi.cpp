@@ -635,14 +635,18 @@ extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t
   return NQPU_OK;
 }
 
+static bool mode_ok(NqpuMode mode) {
+  return mode == NQPU_MODE_TILED || mode == NQPU_MODE_PERGATE || mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR ||
+         mode == NQPU_MODE_AUTO;
+}
+
 extern "C" NqpuError nqpu_circuit_execute_ex(const NqpuCircuit* circuit, NqpuState* state, NqpuMode mode) {
   if (!circuit) return NQPU_NULL_POINTER;
   if (!state) return NQPU_NULL_POINTER;
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;  // c_ffi.rs:1360
-  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED && mode != NQPU_MODE_TENSOR)
-    return NQPU_INVALID_PARAMETER;
+  if (!mode_ok(mode)) return NQPU_INVALID_PARAMETER;
   // the fused and tensor modes run complex64 states of >= 12 qubits (5 fused + 7 row bits)
   if ((mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) && (s->dt != DType::C64 || s->n < 12))
     return NQPU_INVALID_PARAMETER;
@@ -658,8 +662,7 @@ extern "C" NqpuError nqpu_circuit_execute_measured(const NqpuCircuit* circuit, N
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;
-  if (mode != NQPU_MODE_TILED && mode != NQPU_MODE_PERGATE && mode != NQPU_MODE_FUSED && mode != NQPU_MODE_TENSOR)
-    return NQPU_INVALID_PARAMETER;
+  if (!mode_ok(mode)) return NQPU_INVALID_PARAMETER;
   if ((mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) && (s->dt != DType::C64 || s->n < 12))
     return NQPU_INVALID_PARAMETER;
   uint32_t nmeas = 0;
@@ -680,6 +683,7 @@ extern "C" NqpuError nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState*
   const CircuitImpl* c = Cc(circuit);
   StateImpl* s = S(state);
   if (c->n > s->n) return NQPU_INVALID_PARAMETER;
+  if (!mode_ok(mode)) return NQPU_INVALID_PARAMETER;
   if ((mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) && (s->dt != DType::C64 || s->n < 12))
     return NQPU_INVALID_PARAMETER;
   std::vector<cudaEvent_t> ev;
@@ -716,6 +720,7 @@ extern "C" NqpuError nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_
   if (len < 3) return NQPU_INVALID_PARAMETER;
   const CircuitImpl* c = Cc(circuit);
   if (num_qubits < c->n || num_qubits > uint32_t(kMaxQubits)) return NQPU_INVALID_PARAMETER;
+  if (!mode_ok(mode)) return NQPU_INVALID_PARAMETER;
   PlanStats st;
   if (!circuit_plan_stats(c, num_qubits, dtype == NQPU_C64 ? DType::C64 : DType::C128, int(mode), &st))
     return NQPU_INVALID_PARAMETER;
@@ -723,6 +728,18 @@ extern "C" NqpuError nqpu_circuit_plan_stats(const NqpuCircuit* circuit, uint32_
   out[1] = st.ops;
   out[2] = st.stages;
   if (len >= 4) out[3] = st.upload_bytes;
+  return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_circuit_auto_mode(const NqpuCircuit* circuit, uint32_t num_qubits, NqpuDtype dtype,
+                                            NqpuMode* out) {
+  if (!circuit || !out) return NQPU_NULL_POINTER;
+  const CircuitImpl* c = Cc(circuit);
+  if (num_qubits < c->n || num_qubits > uint32_t(kMaxQubits)) return NQPU_INVALID_PARAMETER;
+  const Segment seg = circuit_segments(c->gates).front();
+  const std::vector<Op> ops =
+      lower_circuit(std::vector<GateRec>(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end)));
+  *out = NqpuMode(auto_mode_for(ops, num_qubits, dtype == NQPU_C64 ? DType::C64 : DType::C128));
   return NQPU_OK;
 }
 

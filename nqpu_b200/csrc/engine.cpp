@@ -8,6 +8,7 @@
 #include "device_once.h"
 #include "fused.h"
 #include "kernels.h"
+#include "tcpass.h"
 #include "tcrun.h"
 
 namespace nqpu {
@@ -284,11 +285,62 @@ static bool plan_host(const CircuitImpl* c, const Segment& seg, uint32_t n, DTyp
   return true;
 }
 
+// NQPU_MODE_AUTO: a device-time model in units of one HBM pass over the
+// state (2 S bytes; every cost below scales with 2^n, so the choice does not
+// depend on n).  Tiled passes: one unit per pass plus the shared-memory tile
+// work of each op (dense 1-qubit 0.15, dense 2-qubit 0.30, diagonal 0.058,
+// permutations free: they are deferred into the write-back addresses).
+// Tensor passes: one unit per pass plus 0.35 per fused unitary (its MMAs and
+// epilogue on every tile).  The coefficients are fits to 30-qubit complex64
+// runs of the brickwork (tiled 69 passes / 1200 U3, tensor 81 passes / 178
+// unitaries) and of the QFT (tiled 8 passes / 30 H + 435 controlled phases)
+// against the copy time of the state.  The tensor mode is taken when its
+// model is at least 10 % below the tiled one.
+int auto_mode_for(const std::vector<Op>& ops, uint32_t n, DType dt) {
+  if (dt != DType::C64 || int(n) < kTcMinQubits) return NQPU_MODE_TILED;
+  PlanStats ts;
+  if (!tc_plan_stats(ops, int(n), dt, &ts)) return NQPU_MODE_TILED;
+  TilePlan tp;
+  std::string err;
+  if (!build_tile_plan(ops, int(n), dt, tile_kmax_for(dt), &tp, &err)) return NQPU_MODE_TENSOR;
+  double work = 0.0;
+  for (const Op& op : ops) {
+    switch (op.kind) {
+      case OP_U1: work += 0.15; break;
+      case OP_U2: work += 0.30; break;
+      case OP_D1:
+      case OP_D2:
+      case OP_PH: work += 0.058; break;
+      default: break;  // OP_X1, OP_SW
+    }
+  }
+  const double tiled = double(tp.stats.passes) + work;
+  const double tensor = double(ts.passes) + 0.35 * double(ts.stages);
+  return tensor < 0.9 * tiled ? NQPU_MODE_TENSOR : NQPU_MODE_TILED;
+}
+
+static std::vector<Op> segment_ops(const CircuitImpl* c, const Segment& seg) {
+  return lower_circuit(std::vector<GateRec>(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end)));
+}
+
 bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out) {
   *out = PlanStats{};
   for (const Segment& seg : circuit_segments(c->gates)) {
     DevicePlan p;
     PlanStats st;
+    if (mode == NQPU_MODE_AUTO) {
+      if (seg.begin == seg.end) continue;
+      const int m = auto_mode_for(segment_ops(c, seg), n, dt);
+      CircuitImpl one;
+      one.n = c->n;
+      one.gates.assign(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end));
+      if (!circuit_plan_stats(&one, n, dt, m, &st)) return false;
+      out->passes += st.passes;
+      out->ops += st.ops;
+      out->stages += st.stages;
+      out->upload_bytes += st.upload_bytes;
+      continue;
+    }
     if (mode == NQPU_MODE_FUSED || mode == NQPU_MODE_TENSOR) {
       p.ops = lower_circuit(std::vector<GateRec>(c->gates.begin() + long(seg.begin), c->gates.begin() + long(seg.end)));
       const bool ok = mode == NQPU_MODE_FUSED ? fused_plan_stats(p.ops, int(n), dt, &st)
@@ -379,6 +431,11 @@ cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode, std::vector<cuda
 static cudaError_t segment_run(CircuitImpl* c, const Segment& seg, int si, StateImpl* s, int mode,
                                std::vector<cudaEvent_t>* events) {
   if (seg.begin == seg.end) return cudaSuccess;
+  if (mode == NQPU_MODE_AUTO) {
+    std::pair<uint64_t, int>& am = c->auto_modes[std::make_tuple(s->n, int(s->dt), si)];
+    if (am.first != c->version + 1) am = {c->version + 1, auto_mode_for(segment_ops(c, seg), s->n, s->dt)};
+    mode = am.second;
+  }
   const int effective = (mode == NQPU_MODE_TILED && int(s->n) < tile_min_qubits(s->dt)) ? int(NQPU_MODE_PERGATE) : mode;
   const auto key = std::make_tuple(s->n, int(s->dt), effective, si);
   DevicePlan*& p = c->plans[key];

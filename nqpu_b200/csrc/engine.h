@@ -66,6 +66,9 @@ struct CircuitImpl {
   // cached plans per (state qubits, dtype, mode, segment); segments are the
   // gate runs between mid-circuit measurements / resets
   std::map<std::tuple<uint32_t, int, int, int>, DevicePlan*> plans;
+  // NQPU_MODE_AUTO's choice per (state qubits, dtype, segment): (circuit
+  // version + 1, mode); version + 1 so that a default entry reads as unset
+  std::map<std::tuple<uint32_t, int, int>, std::pair<uint64_t, int>> auto_modes;
   std::mutex mu;
 };
 
@@ -91,6 +94,8 @@ cudaError_t circuit_run(CircuitImpl* c, StateImpl* s, int mode,
                         std::vector<cudaEvent_t>* events = nullptr,
                         std::vector<uint32_t>* outcomes = nullptr);
 bool circuit_plan_stats(const CircuitImpl* c, uint32_t n, DType dt, int mode, PlanStats* out);
+// The mode NQPU_MODE_AUTO runs a lowered gate run in on an n-qubit state.
+int auto_mode_for(const std::vector<Op>& ops, uint32_t n, DType dt);
 
 // Run a lowered op list on a state with the given mode (used by batch/server).
 cudaError_t run_ops_pergate(StateImpl* s, const std::vector<Op>& ops);

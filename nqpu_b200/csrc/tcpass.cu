@@ -3,25 +3,31 @@
 // in shared memory (plan data and layouts in tcpass.h, planner in tcplan.cpp).
 //
 // Per pass, one persistent CTA per SM with four independent tile engines of
-// eight warps.  An engine owns an operand buffer (the tile as the 128 x 64
-// FP16 A operand: hi and lo planes, K-major, 128-byte swizzle, 32 KB) and a
-// 128-column TMEM accumulator, and runs its tiles through:
-//   load     8 coalesced 16-byte HBM loads per thread (a tile = 128 runs of
-//            32 amplitudes), scale by s (a power of two, for the FP16 range)
-//            and the renormalisation factor, split x = hi + lo into FP16
-//            pairs and store them into the operand in unitary 0's layout;
+// four warps (one per TMEM lane quadrant).  An engine owns an operand buffer
+// (the tile as the 128 x 64 FP16 A operand: hi and lo planes, K-major,
+// 128-byte swizzle, 32 KB) and a 128-column TMEM accumulator, and runs its
+// tiles through:
+//   load     the tile's 32 KB (128 runs of 32 contiguous amplitudes) arrive
+//            by 16-byte cp.async as raw FP32 in the engine's own operand
+//            buffer; they are issued as soon as the previous tile's last MMAs
+//            are done, so they fly during that tile's last epilogue;
+//   split    each thread reads back its own 16 chunks, the engine meets at a
+//            barrier (the buffer is converted in place), then scales by s (a
+//            power of two, for the FP16 range) and the renormalisation
+//            factor, splits x = hi + lo into FP16 pairs and stores them in
+//            unitary 0's operand layout;
 //   unitary  one elected thread issues 8 MMAs (K = 16): D[:, 0:128] =
 //            A_hi [B_hi; B_lo]^T (N = 128) then D[:, 0:64] += A_lo B_hi^T
 //            (N = 64), B = the real embedding of 16 U, and commits them to
-//            the engine's mbarrier (bounded wait);
-//   epilogue each thread reads half of its row (TMEM lane) of D: warps w and
-//            w + 4 of an engine share a lane quadrant and take 16 columns
-//            each; it forms out = (D[:, 0:64] + D[:, 64:128]) / 16 and either
-//            splits its amplitudes straight into the next unitary's operand
+//            the engine's mbarrier; one warp polls it (bounded) while the
+//            other three wait at the engine's named barrier;
+//   epilogue each thread drains its row (TMEM lane) of D, two 4-column parts
+//            per TMEM load wait, forms out = (D[:, 0:64] + D[:, 64:128]) / 16
+//            and either splits it straight into the next unitary's operand
 //            layout, or, after the last unitary, stores out / s to HBM.
-// While one engine waits for its MMAs or its loads the other three run, so
-// the tensor pipe, shared memory and HBM overlap across four tiles.  The B
-// operands of the pass's unitaries stay in shared memory for the launch.
+// While one engine waits for its MMAs the other three run, so the tensor
+// pipe, shared memory and HBM overlap across four tiles.  The B operands of
+// the pass's unitaries stay in shared memory for the launch.
 //
 // Renormalisation: the first pass of a run records the FP64 norm of its input
 // (per-CTA partials) and every pass the norm of its output; each later pass
@@ -44,23 +50,39 @@
 
 namespace nqpu {
 
+// An engine is one warp per TMEM lane quadrant (4 warps, 128 threads): each
+// thread drains whole rows, so 512 threads per CTA with up to 128 registers
+// each.  (Measured on the 30-qubit brickwork against 8-warp engines with two
+// warps per quadrant at 64 registers: 2-3.5 % faster.)
 constexpr int kTcEngines = 4;
-constexpr int kTcEngineThreads = 256;
+constexpr int kTcEngineWarps = 4;
+constexpr int kTcEngineThreads = 32 * kTcEngineWarps;
 constexpr int kTcThreads = kTcEngines * kTcEngineThreads;
-constexpr int kTcLoadSteps = 1 << kTcLoadStepBits;   // 16-byte loads per thread per tile
-static_assert((1 << kTcLoadThreadBits) == kTcEngineThreads, "one loading thread per engine thread");
-static_assert(kTcLoadThreadBits + kTcLoadStepBits == kTcTileBits - 1, "loads cover the tile");
+constexpr int kTcThrBits = kTcLoadThreadBits;                 // loader: thread bits of an engine
+constexpr int kTcStpBits = kTcLoadStepBits;                   // loader: step bits
+static_assert((1 << kTcThrBits) == kTcEngineThreads, "one loading thread per engine thread");
+static_assert(kTcThrBits + kTcStpBits == kTcTileBits - 1, "loads cover the tile");
+constexpr int kTcLoadSteps = 1 << kTcStpBits;                 // 16-byte chunks per thread per tile
+constexpr int kTcColHalves = kTcEngineWarps / 4;              // warps sharing a lane quadrant
+constexpr int kTcCols = 32 / kTcColHalves;                    // complex columns a thread drains
+constexpr int kTcParts = kTcCols / 4;                         // epilogue parts of 4 columns
+constexpr int kTcBatch = 2;                                   // parts per TMEM load wait (4: spills)
+static_assert(kTcParts % kTcBatch == 0, "whole batches");
 constexpr uint32_t kTcAPlane = 128 * 128;            // 16 KB: 128 rows x 64 halves
 constexpr uint32_t kTcOpBytes = 2 * kTcAPlane;       // hi + lo planes
 constexpr uint32_t kTcBBytes = 128 * 128;            // [B_hi; B_lo]: 128 rows x 64 halves
 constexpr uint32_t kTcWaitLimit = 1u << 22;          // bounded mbarrier polls
 constexpr uint32_t kTcTmemCols = 512;                // four engines x one 128-column accumulator
 
+// Every offset the kernel forms is GF(2)-linear in the bits of its index (the
+// swizzled operand layout XORs disjoint fields; amplitude offsets OR disjoint
+// qubit bits), so the tables hold one entry per index bit and the kernel
+// combines them with XORs / adds of compile-time selections.
 struct TcTables {
-  uint32_t xnext[kTcMaxUnitaries][32];
-  uint64_t gcol[kTcMaxUnitaries][32];
-  uint32_t sol[kTcLoadSteps];  // loader: operand offset (unitary 0's layout) of load step i
-  uint64_t sgl[kTcLoadSteps];  // loader: amplitude offset of load step i
+  uint32_t xcb[kTcMaxUnitaries][5];  // epilogue of unitary j: next-layout operand offset of column bit i
+  uint64_t gcb[kTcMaxUnitaries][5];  // epilogue of the last unitary: amplitude offset of column bit i
+  uint32_t sob[kTcStpBits];          // loader: operand offset (unitary 0's layout) of step bit s
+  uint64_t sgb[kTcStpBits];          // loader: amplitude offset of step bit s
 };
 
 constexpr size_t kTcSmem = 1024 /*alignment*/ + kTcEngines * size_t(kTcOpBytes) +
@@ -73,6 +95,20 @@ constexpr uint32_t kIdescN64 = umma_idesc_f16<128, 64>();
 __device__ __forceinline__ void engine_sync(int e) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(1 + e), "n"(kTcEngineThreads) : "memory");
 }
+
+__device__ __forceinline__ float4 lds_v4(uint32_t addr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(addr)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void cp_async16_s(uint32_t saddr, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // FP16 hi/lo split of an (re, im) pair: hi = half(x), lo = half(x - hi)
 // (x - hi is exact in FP32; one packed FP32x2 FMA), as two packed half2 words.
@@ -99,11 +135,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __shared__ __align__(8) uint64_t mbar[kTcEngines];
   __shared__ uint32_t tmem_holder;
   __shared__ int s_abort[kTcEngines];
+  __shared__ float s_scale_in;
   __shared__ double s_red[2][kTcThreads / 32];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int e = tid / kTcEngineThreads, et = tid % kTcEngineThreads;
-  const int q = warp & 3, ch = (warp >> 2) & 1;  // TMEM lane quadrant, column half
+  const int q = warp & 3, ch = (et >> 7) & (kTcColHalves - 1);  // TMEM lane quadrant, column half
   const uint32_t row = uint32_t(32 * q + lane);  // this thread's operand row = its TMEM lane
 
   // ---- prologue: pass record, B operands, tables, barriers, TMEM ----
@@ -123,20 +160,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       *reinterpret_cast<uint4*>(bdst + tc_sw128_off(nrow, k)) = __ldg(bsrc + i);
     }
   }
-  for (int i = tid; i < m * 32; i += kTcThreads) {
-    T->xnext[i >> 5][i & 31] = P.u[i >> 5].xnext[i & 31];
-    T->gcol[i >> 5][i & 31] = P.u[i >> 5].gcol[i & 31];
+  if (tid < 5 * m) {
+    const int j = tid / 5, i = tid % 5;
+    T->xcb[j][i] = j + 1 < m ? P.u[j + 1].boff[P.u[j].fcol[i]] : 0u;
+    T->gcb[j][i] = 1ull << P.qt[P.u[j].fcol[i]];
   }
-  if (tid < kTcLoadSteps) {
-    uint32_t o = 0;
-    uint64_t a = 0;
-    for (int s = 0; s < kTcLoadStepBits; ++s)
-      if ((tid >> s) & 1) {
-        o ^= P.u[0].boff[P.lt[kTcLoadThreadBits + s]];
-        a |= 1ull << P.qt[P.lt[kTcLoadThreadBits + s]];
-      }
-    T->sol[tid] = o;
-    T->sgl[tid] = a;
+  if (tid < kTcStpBits) {
+    T->sob[tid] = P.u[0].boff[P.lt[kTcThrBits + tid]];
+    T->sgb[tid] = 1ull << P.qt[P.lt[kTcThrBits + tid]];
   }
   const uint32_t mbar_s = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar[0]));
   if (tid < kTcEngines) {
@@ -149,6 +180,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                  "r"(kTcTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
+  if (warp == 1) {
+    // renormalisation factor of this pass's input, times the operand scale s:
+    // one warp sums the per-CTA partials in a fixed order (every CTA gets the
+    // same factor) and shares it
+    float sc = state_scale;
+    if (prev_norm && norm0) {
+      double t0 = 0.0, tp = 0.0;
+      for (int i = lane; i < n_prev; i += 32) {
+        t0 += norm0[i];
+        tp += prev_norm[i];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        t0 += __shfl_xor_sync(0xffffffffu, t0, o);
+        tp += __shfl_xor_sync(0xffffffffu, tp, o);
+      }
+      if (t0 > 0.0 && tp > 0.0) sc = float(double(state_scale) * sqrt(t0 / tp));
+    }
+    if (lane == 0) s_scale_in = sc;
+  }
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   fence_proxy_async_smem();  // the B operands, written by generic stores, are read by the tensor core
   tc_fence_before();
@@ -156,25 +207,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
 
-  // renormalisation factor of this pass's input, times the operand scale s
-  float scale_in = state_scale;
-  if (prev_norm && norm0) {
-    double t0 = 0.0, tp = 0.0;
-    for (int i = 0; i < n_prev; ++i) {
-      t0 += norm0[i];
-      tp += prev_norm[i];
-    }
-    if (t0 > 0.0 && tp > 0.0) scale_in = float(double(state_scale) * sqrt(t0 / tp));
-  }
+  const float scale_in = s_scale_in;
   const float mid_scale = 1.0f / kTcUScale;                       // exact: a power of two
   const float out_scale = 1.0f / (kTcUScale * state_scale);       // exact: a power of two
 
   // ---- per-thread address parts ----
   // loader: thread bit b of et is tile bit lt[b], step bit s is tile bit
-  // lt[kTcLoadThreadBits + s], and tile bit 0 is the pair inside each 16-byte load
+  // lt[kTcThrBits + s], and tile bit 0 is the pair inside each 16-byte load
   uint32_t pol = 0;
   uint64_t pgl = 0;
-  for (int b = 0; b < kTcLoadThreadBits; ++b)
+  for (int b = 0; b < kTcThrBits; ++b)
     if ((et >> b) & 1) {
       pol ^= P.u[0].boff[P.lt[b]];
       pgl |= 1ull << P.qt[P.lt[b]];
@@ -205,7 +247,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t b_s = static_cast<uint32_t>(__cvta_generic_to_shared(bbuf));
   const uint32_t my_mbar = mbar_s + 8u * uint32_t(e);
   const uint32_t acc = tmem + 128u * uint32_t(e);
-  const uint32_t lanes = acc + (uint32_t(q * 32) << 16) + 32u * uint32_t(ch);
+  const uint32_t lanes = acc + (uint32_t(q * 32) << 16) + uint32_t(2 * kTcCols * ch);
 
   auto tile_base_of = [&](uint32_t tile) {
     const uint64_t mine = (lane < P.n_out && ((tile >> lane) & 1u)) ? (1ull << P.qout[lane]) : 0ull;
@@ -232,25 +274,54 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     engine_sync(e);
     tc_fence_after();
   };
+  // raw FP32 chunks of `tile` into the engine's operand buffer by 16-byte
+  // cp.async: this thread's chunk of step i at raw_part + 16 i (threads of
+  // the engine); each thread reads back only its own chunks
+  const uint32_t raw_part = 16u * uint32_t(et);
+  auto issue_loads = [&](uint32_t tile) {
+    const uint64_t tbn = tile_base_of(tile);
+    const float4* src = reinterpret_cast<const float4*>(amp) + ((tbn + pgl) >> 1);
+    uint64_t sgb[kTcStpBits];
+#pragma unroll
+    for (int b = 0; b < kTcStpBits; ++b) sgb[b] = T->sgb[b] >> 1;  // in 16-byte chunks
+#pragma unroll
+    for (int i = 0; i < kTcLoadSteps; ++i) {
+      uint64_t a = 0;
+#pragma unroll
+      for (int b = 0; b < kTcStpBits; ++b)
+        if ((i >> b) & 1) a += sgb[b];
+      cp_async16_s(ahi_s + raw_part + 16u * uint32_t(i * kTcEngineThreads), src + a);
+    }
+    cp_async_commit();
+  };
 
   double norm_in = 0.0, norm_out = 0.0;
   uint32_t phase = 0;  // parity of the engine's mbarrier phase to wait for
   const uint32_t stride = uint32_t(kTcEngines) * gridDim.x;
-  for (uint32_t tile = uint32_t(kTcEngines) * blockIdx.x + uint32_t(e); tile < n_tiles; tile += stride) {
+  const uint32_t first_tile = uint32_t(kTcEngines) * blockIdx.x + uint32_t(e);
+  if (first_tile < n_tiles) issue_loads(first_tile);
+  for (uint32_t tile = first_tile; tile < n_tiles; tile += stride) {
     const uint64_t tb = tile_base_of(tile);
     // ---- load, scale, split into unitary 0's operand ----
     {
       float4 v[kTcLoadSteps];
-      const float4* src = reinterpret_cast<const float4*>(amp) + ((tb + pgl) >> 1);
+      cp_async_wait0();
 #pragma unroll
-      for (int i = 0; i < kTcLoadSteps; ++i) v[i] = __ldcs(src + (T->sgl[i] >> 1));
+      for (int i = 0; i < kTcLoadSteps; ++i) v[i] = lds_v4(ahi_s + raw_part + 16u * uint32_t(i * kTcEngineThreads));
+      uint32_t sob[kTcStpBits];
+#pragma unroll
+      for (int b = 0; b < kTcStpBits; ++b) sob[b] = T->sob[b];
+      engine_sync(e);  // every raw chunk is in registers before the operand overwrites the buffer
       const float2 s2 = make_float2(scale_in, scale_in);
       float2 nin = make_float2(0.0f, 0.0f);  // FP32 partials over this thread's amplitudes, FP64 across tiles
 #pragma unroll
       for (int i = 0; i < kTcLoadSteps; ++i) {
         const float2 x0 = make_float2(v[i].x, v[i].y), x1 = make_float2(v[i].z, v[i].w);
         if (norm0_out) nin = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nin));
-        const uint32_t o = pol ^ T->sol[i];
+        uint32_t o = pol;
+#pragma unroll
+        for (int b = 0; b < kTcStpBits; ++b)
+          if ((i >> b) & 1) o ^= sob[b];
         if (load_pair) {
           put2(o, __fmul2_rn(x0, s2), __fmul2_rn(x1, s2));
         } else {
@@ -276,7 +347,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dlo + 2u * kk, dbj + 2u * kk, kIdescN64, 1u);
         umma_commit(my_mbar);
       }
-      {
+      if (et < 32) {
+        // one warp polls the mbarrier; the engine's other warps wait at the
+        // named barrier below without taking issue slots
         uint32_t it = 0;
         bool done = false;
         while (!(done = mbar_try_wait(my_mbar, phase)) && ++it < kTcWaitLimit) {
@@ -289,6 +362,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           for (uint32_t w = 0; w < 4 * kTcWaitLimit && !mbar_try_wait(my_mbar, phase); ++w) {
           }
         }
+        tc_fence_before();
+      }
+      {
         engine_sync(e);
         phase ^= 1u;
         if (s_abort[e]) {
@@ -299,6 +375,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       // ---- epilogue of unitary j ----
       const bool last = j + 1 == m;
+      // the last MMAs are done, so the operand buffer is free: the next tile's
+      // copies fly while this tile's epilogue stores to HBM
+      if (last && tile + stride < n_tiles) issue_loads(tile + stride);
       uint32_t my_ptn = 0;
       bool my_pair = false;
 #pragma unroll
@@ -307,41 +386,72 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           my_ptn = ptn[jj];
           my_pair = pair[jj];
         }
-      float2* out = reinterpret_cast<float2*>(amp) + (tb + pg);
+      // column c = kTcCols ch + 4 part + cc (+ 1 for the second amplitude of
+      // a pair): its offsets are the XOR (operand) / sum (amplitude) of one
+      // table entry per set bit
+      uint32_t xb[5];
+      uint64_t gb[5];
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        xb[i] = T->xcb[j][i];
+        gb[i] = last ? T->gcb[j][i] : 0ull;
+      }
+      uint32_t xbase = my_ptn;
+      uint64_t gbase = tb + pg;
+      if (kTcColHalves == 2 && ch) {
+        xbase ^= xb[4];
+        gbase += gb[4];
+      }
+      float2* out = reinterpret_cast<float2*>(amp) + gbase;
       float2 nout = make_float2(0.0f, 0.0f);
       const float scv = last ? out_scale : mid_scale;
       const float2 sc = make_float2(scv, scv);
 #pragma unroll
-      for (int part = 0; part < 4; ++part) {
-        uint32_t rh[8], rl[8];
-        tmem_ld8(lanes + 8u * uint32_t(part), rh);
-        tmem_ld8(lanes + 64u + 8u * uint32_t(part), rl);
+      for (int pb = 0; pb < kTcParts; pb += kTcBatch) {
+        uint32_t rh[kTcBatch][8], rl[kTcBatch][8];
+#pragma unroll
+        for (int k = 0; k < kTcBatch; ++k) {
+          tmem_ld8(lanes + 8u * uint32_t(pb + k), rh[k]);
+          tmem_ld8(lanes + 64u + 8u * uint32_t(pb + k), rl[k]);
+        }
         tmem_ld_wait();
 #pragma unroll
-        for (int cc = 0; cc < 4; cc += 2) {
-          const int c = 16 * ch + 4 * part + cc;
-          // out = (D[:, 0:64] + D[:, 64:128]) * scale, packed (re, im)
-          const float2 x0 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[2 * cc]), __uint_as_float(rh[2 * cc + 1])),
-                                                  make_float2(__uint_as_float(rl[2 * cc]), __uint_as_float(rl[2 * cc + 1]))),
-                                       sc);
-          const float2 x1 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[2 * cc + 2]), __uint_as_float(rh[2 * cc + 3])),
-                                                  make_float2(__uint_as_float(rl[2 * cc + 2]), __uint_as_float(rl[2 * cc + 3]))),
-                                       sc);
-          if (!last) {
-            const uint32_t o0 = my_ptn ^ T->xnext[j][c];
-            if (my_pair) {
-              put2(o0, x0, x1);
+        for (int k = 0; k < kTcBatch; ++k) {
+#pragma unroll
+          for (int cc = 0; cc < 4; cc += 2) {
+            const int cb = 4 * (pb + k) + cc;  // column bits below the column half (compile time)
+            uint32_t xo = 0;
+            uint64_t go = 0;
+#pragma unroll
+            for (int b = 1; b < 5; ++b)
+              if ((cb >> b) & 1) {
+                xo ^= xb[b];
+                go += gb[b];
+              }
+            // out = (D[:, 0:64] + D[:, 64:128]) * scale, packed (re, im)
+            const float2 x0 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[k][2 * cc]), __uint_as_float(rh[k][2 * cc + 1])),
+                                                    make_float2(__uint_as_float(rl[k][2 * cc]), __uint_as_float(rl[k][2 * cc + 1]))),
+                                         sc);
+            const float2 x1 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[k][2 * cc + 2]), __uint_as_float(rh[k][2 * cc + 3])),
+                                                    make_float2(__uint_as_float(rl[k][2 * cc + 2]), __uint_as_float(rl[k][2 * cc + 3]))),
+                                         sc);
+            if (!last) {
+              const uint32_t o0 = xbase ^ xo;
+              if (my_pair) {
+                put2(o0, x0, x1);
+              } else {
+                put1(o0, x0);
+                put1(o0 ^ xb[0], x1);
+              }
             } else {
-              put1(o0, x0);
-              put1(my_ptn ^ T->xnext[j][c + 1], x1);
-            }
-          } else {
-            nout = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nout));
-            if (store16) {
-              __stcs(reinterpret_cast<float4*>(out + T->gcol[j][c]), make_float4(x0.x, x0.y, x1.x, x1.y));
-            } else {
-              __stcs(out + T->gcol[j][c], x0);
-              __stcs(out + T->gcol[j][c + 1], x1);
+              nout = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nout));
+              float2* o0 = out + go;
+              if (store16) {
+                __stcs(reinterpret_cast<float4*>(o0), make_float4(x0.x, x0.y, x1.x, x1.y));
+              } else {
+                __stcs(o0, x0);
+                __stcs(o0 + gb[0], x1);
+              }
             }
           }
         }
@@ -352,6 +462,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     if (aborted) break;
   }
+
+  cp_async_wait0();  // no copy outlives the CTA (an aborted engine may leave one in flight)
 
   // ---- per-CTA FP64 norm partials (fixed-order reduction), teardown ----
   tc_fence_before();
@@ -433,7 +545,7 @@ bool tc_plan_stats(const std::vector<Op>& ops, int n, DType dt, PlanStats* stats
   if (dt != DType::C64) return false;
   TcPlan tp;
   std::string err;
-  if (!build_tc_plan(ops, n, &tp, &err)) return false;
+  if (!build_tc_plan(ops, n, &tp, &err, false)) return false;
   *stats = tp.stats;
   return true;
 }

@@ -27,8 +27,8 @@ constexpr int kTcTileBits = 12;
 constexpr int kTcLowBits = 5;        // tile bits 0..4 = qubits 0..4
 constexpr int kTcMaxUnitaries = 3;   // per pass (their B operands stay in shared memory)
 constexpr int kTcMinQubits = 12;
-constexpr int kTcLoadThreadBits = 8; // loading threads per tile engine: 256
-constexpr int kTcLoadStepBits = 3;   // 16-byte loads per thread: 8
+constexpr int kTcLoadThreadBits = 7; // loading threads per tile engine: 128
+constexpr int kTcLoadStepBits = 4;   // 16-byte chunks per thread: 16
 // The unitaries are stored as 16 U (entries up to 16 in magnitude keep their
 // small entries clear of the FP16 subnormal range); epilogues divide by 16.
 constexpr float kTcUScale = 16.0f;
@@ -90,6 +90,8 @@ float tc_half_value(uint16_t h);
 float tc_state_scale(int n);
 
 // Plan a lowered op list for the tensor-core pass mode (complex64, n >= 12).
-bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err);
+// With finish = false only the pass and unitary structure is built (stats,
+// pass qubits and clusters), not the layouts, offset tables or B operands.
+bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err, bool finish = true);
 
 }  // namespace nqpu

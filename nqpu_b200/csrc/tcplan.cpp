@@ -98,16 +98,18 @@ int layout_cost(const LayoutCfg& c, int m, const int* qt) {
   uint32_t boff[kTcMaxUnitaries][12];
   for (int j = 0; j < m; ++j) layout_offsets(c.frow[j], c.fcol[j], boff[j]);
   int cost = 0;
-  // loader: 8 warps x 8 steps, lanes over tile bits lt[0..4], hi and lo
+  // loader: 64 warp-steps per tile (4 warps x 16 steps), lanes over tile
+  // bits lt[0..4], hi and lo
   // planes; the two amplitudes of a 16-byte load are one 8-byte store when
   // tile bit 0 is column bit 0 of unitary 0, else two 4-byte stores
   if (c.fcol[0][0] == 0) cost += 64 * 2 * store_wavefronts(c.lt, boff[0], 8);
   else cost += 64 * 2 * 2 * store_wavefronts(c.lt, boff[0], 4);
-  // epilogue: 8 warps x 16 columns, pairs of columns as 8-byte stores when
+  // epilogue: 4 warps x 32 columns (128 column-stores per tile, or 256
+  // single ones), pairs of columns as 8-byte stores when
   // both layouts share column bit 0
   for (int j = 0; j + 1 < m; ++j) {
     const bool pair = c.fcol[j][0] == c.fcol[j + 1][0];
-    cost += 8 * (pair ? 8 : 16) * 2 * store_wavefronts(c.frow[j], boff[j + 1], pair ? 8 : 4);
+    cost += 4 * (pair ? 16 : 32) * 2 * store_wavefronts(c.frow[j], boff[j + 1], pair ? 8 : 4);
   }
   // HBM: lanes over rows 0..4 of the last layout.  A 32-byte sector holds the
   // 4 amplitudes that differ in qubits 0 and 1 (tile bits 0 and 1), so a warp
@@ -119,7 +121,7 @@ int layout_cost(const LayoutCfg& c, int m, const int* qt) {
   int k = 0;
   for (int i = 0; i < 5; ++i) k += (c.frow[L][i] == 0 || c.frow[L][i] == 1) ? 1 : 0;
   const int ns = 32 >> k, ideal = wide ? 16 : 8;
-  cost += (8 * (wide ? 8 : 16) * (ns - ideal)) / 4;
+  cost += (4 * (wide ? 16 : 32) * (ns - ideal)) / 4;
   return cost;
 }
 
@@ -278,7 +280,7 @@ float tc_state_scale(int n) {
   return float(1u << e);
 }
 
-bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err) {
+bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* err, bool finish) {
   out->n = n;
   out->state_scale = tc_state_scale(n);
   out->passes.clear();
@@ -372,6 +374,12 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     for (auto& cl : clusters) cluster_ops.push_back(std::move(cl.second));
     out->stats.stages += uint64_t(P.m);
     remaining.swap(rest);
+  }
+  if (!finish) {
+    out->stats.passes = out->passes.size();
+    out->stats.ops = ops.size();
+    out->stats.upload_bytes = out->passes.size() * sizeof(TcPassRec) + out->stats.stages * kTcBmatHalves * sizeof(uint16_t);
+    return true;
   }
   // ---- per pass (independent, on host threads): layouts, offset tables,
   // unitaries and their split real embeddings ----

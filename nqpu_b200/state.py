@@ -16,7 +16,7 @@ from ._lib import NqpuComplex, NqpuMeasurement, check
 from .circuits import ARITY, MID_GATES, NPARAMS
 
 C128, C64 = 0, 1
-MODES = {"tiled": 0, "pergate": 1, "fused": 2, "tensor": 3}
+MODES = {"tiled": 0, "pergate": 1, "fused": 2, "tensor": 3, "auto": 4}
 DTYPES = {"c128": C128, "complex128": C128, "c64": C64, "complex64": C64}
 
 

@@ -126,6 +126,20 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
       }
       if (P.lt[0] != 1 || P.lt[1] != 2 || P.lt[2] != 3) return -5;
     }
+    // the kernel forms the epilogue offsets from one entry per column bit:
+    // xnext and gcol must be linear (XOR of the next layout's offsets, sum of
+    // the qubits' amplitude strides) in the bits of the column index
+    for (int j = 0; j < m; ++j)
+      for (uint32_t c = 0; c < 32; ++c) {
+        uint32_t x = 0;
+        uint64_t g = 0;
+        for (int i = 0; i < 5; ++i)
+          if ((c >> i) & 1u) {
+            if (j + 1 < m) x ^= P.u[j + 1].boff[P.u[j].fcol[i]];
+            g += 1ull << P.qt[P.u[j].fcol[i]];
+          }
+        if ((j + 1 < m && P.u[j].xnext[c] != x) || (j + 1 == m && P.u[j].gcol[c] != g)) return -4;
+      }
     const uint32_t boff_h = P.u[0].boff[0];
     const bool load_pair = boff_h == 4u;  // tile bit 0 is column bit 0 of unitary 0
     const bool store16 = P.qt[P.u[m - 1].fcol[0]] == 0;

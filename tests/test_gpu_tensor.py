@@ -140,3 +140,24 @@ def test_rejects_complex128_and_small_states():
     c = Circuit(12, circuits.brickwork(12, 2, 1))
     with StateVector(12, "c128") as sv, pytest.raises(NqpuErrorException):
         c.execute(sv, "tensor")
+
+
+@pytest.mark.parametrize("n,kind,dtype", [(20, "brickwork", "c64"), (20, "qft", "c64"), (16, "tfim", "c64"),
+                                          (18, "brickwork", "c128"), (10, "brickwork", "c64")])
+def test_auto_mode_matches_oracle(n, kind, dtype):
+    """NQPU_MODE_AUTO runs each gate run in the mode its model picks; the
+    result must meet that dtype's tolerance against the FP64 oracle."""
+    gates = {"brickwork": lambda: circuits.brickwork(n, 12, 5), "qft": lambda: circuits.qft(n),
+             "tfim": lambda: circuits.tfim_trotter(n, 6, 3)[0]}[kind]()
+    rng = np.random.default_rng(n)
+    init = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    init /= np.linalg.norm(init)
+    ref, zref = oracle(n, gates, init)
+    sv = StateVector(n, dtype)
+    sv.set_amplitudes(init)
+    Circuit(n, gates).execute(sv, "auto")
+    got, z = sv.amplitudes(), sv.expectation_z_all()
+    sv.close()
+    tol = TOL if dtype == "c64" else 1e-12
+    assert 1 - fid(ref, got) <= tol
+    assert np.abs(z - zref).max() <= max(tol, 1e-12)
