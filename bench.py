@@ -587,8 +587,33 @@ def run_precision(args):
     clk = clocks.stop()
     sv128, rec128, l128 = run("c128", "tiled")
     f = sv64.fidelity(sv128)
-    errs = [{"step": every * (i + 1), "max_abs_dZ": float(np.abs(a[0] - b[0]).max()), "abs_dZ0Z1": abs(a[1] - b[1])}
-            for i, (a, b) in enumerate(zip(rec64, rec128))]
+
+    def checkpoints(rec):
+        return [{"step": every * (i + 1), "max_abs_dZ": float(np.abs(a[0] - b[0]).max()), "abs_dZ0Z1": abs(a[1] - b[1])}
+                for i, (a, b) in enumerate(zip(rec, rec128))]
+
+    errs = checkpoints(rec64)
+    # the same circuit through the tensor-core pass mode (several fused
+    # unitaries per HBM pass, split FP16) and the engine's own mode choice
+    am = C.c_int(-1)
+    _lib.check(lib.nqpu_circuit_auto_mode(c.h_, n, 1, C.byref(am)), "auto_mode")
+    tensor = None
+    if not args.quick:
+        w = StateVector(n, "c64")
+        c.execute(w, "tensor")  # plan and module load
+        w.close()
+        sv_tc, rec_tc, l_tc = run("c64", "tensor")
+        e_tc = checkpoints(rec_tc)
+        st_tc = c.plan_stats(n, "c64", "tensor")
+        tensor = {"gates_per_s": len(chunk) * (steps // every) / (sum(l_tc) / 1000), "seconds": sum(l_tc) / 1000,
+                  "launches": len(l_tc), "kernel": "k_tc_pass",
+                  "fused_unitaries": st_tc["stages"] * (steps // every),
+                  "hbm_frac": 2 * (1 << n) * 8 / (np.mean(l_tc) / 1000) / 1e9 / peaks()[0],
+                  "accuracy_vs_fp64": {"one_minus_F": 1 - sv_tc.fidelity(sv128),
+                                       "max_abs_dZ": max(e["max_abs_dZ"] for e in e_tc),
+                                       "max_abs_dZ0Z1": max(e["abs_dZ0Z1"] for e in e_tc)},
+                  "engine": MODE_DESCRIPTIONS["tensor"]}
+        sv_tc.close()
     sv128.close()
     plain = None
     if not args.quick:
@@ -648,6 +673,7 @@ def run_precision(args):
                              "max_abs_dZ": max(e["max_abs_dZ"] for e in errs),
                              "max_abs_dZ0Z1": max(e["abs_dZ0Z1"] for e in errs)},
         "fp64_reference_seconds": sum(l128) / 1000, "plain_tiled_c64": plain,
+        "tensor_pass_c64": tensor, "auto_mode_choice": {0: "tiled", 3: "tensor"}.get(am.value, am.value),
         "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": len(l64), "clocks": clk,
     }
     return line
@@ -758,12 +784,10 @@ def run_batch(args):
     e2e = None
     if not args.quick:
         t = time.perf_counter()
-        cs = [Circuit.from_arrays(n, *a) for n, a, _, _ in arrs]
-        t_circ = time.perf_counter()
         b2 = Batch()
         b2.config(**cfg)
-        for c, (n, g, J, h) in zip(cs, items):
-            b2.add_ising(c, J, h)
+        t_circ = time.perf_counter()
+        b2.add_ising_arrays(arrs)  # every circuit's gate arrays in one call
         t_add = time.perf_counter()
         b2.prepare()
         t_prep = time.perf_counter()
@@ -773,11 +797,12 @@ def run_batch(args):
         assert np.array_equal(r2, res)
         e2e = {"value": count / et, "unit": "circuits/s", "h2d_bytes_per_step": int(st["upload_bytes"]),
                "d2h_bytes_per_step": 8 * count, "seconds_per_step": et,
-               "phases_s": {"circuits": t_circ - t, "batch_add": t_add - t_circ, "prepare": t_prep - t_add,
+               "phases_s": {"batch_create": t_circ - t, "batch_add_arrays": t_add - t_circ, "prepare": t_prep - t_add,
                             "run": t_run - t_prep},
+               "prepare_phases_s": b2.stats()["prepare_s"],
                "frac_of_device_rate": (count / et) / value,
-               "timing": "host wall clock: Circuit handles from gate arrays (Circuit.from_arrays), batch add, "
-                         "prepare (plans on host threads, uploads, graph capture), one replay, results on the host"}
+               "timing": "host wall clock: batch from the circuits' gate arrays (one nqpu_batch_add_ising_arrays "
+                         "call), prepare (plans on host threads, uploads, graph capture), one replay, results on the host"}
         b2.close()
         for c in cs:
             c.close()

@@ -361,6 +361,20 @@ void        nqpu_batch_destroy(NqpuBatch* batch);
 /* Append a circuit (5..24 qubits; the gate list is copied) with J[n-1], h[n]. */
 NqpuError   nqpu_batch_add_ising(NqpuBatch* batch, const NqpuCircuit* circuit, const double* J,
                                  const double* h, uint32_t* index);
+/* No counterpart in the reference: the bulk form of nqpu_batch_add_ising
+ * for callers that assemble thousands of circuits (one call instead of two
+ * per circuit, gates checked and copied on host threads).  Circuit i has
+ * num_qubits[i] (5..24) qubits and the gates gate_offsets[i] ..
+ * gate_offsets[i+1]-1 of the flat arrays (the encoding of
+ * nqpu_circuit_add_gates: codes, qubits 3 per gate, params 4 per gate,
+ * matrices 16 per gate or NULL); J and h hold the circuits' n-1 bonds and n
+ * fields one circuit after another.  *first_index = index of circuit 0.
+ * Nothing is added unless every circuit is valid. */
+NqpuError   nqpu_batch_add_ising_arrays(NqpuBatch* batch, uint32_t count, const uint32_t* num_qubits,
+                                        const uint64_t* gate_offsets, const uint32_t* codes,
+                                        const int32_t* qubits, const double* params,
+                                        const NqpuComplex* matrices, const double* J, const double* h,
+                                        uint32_t* first_index);
 NqpuError   nqpu_batch_config(NqpuBatch* batch, NqpuBatchParam param, int32_t value);
 /* Plan every circuit, upload the task queue and capture the CUDA graph
  * (run() does it on first use). */
@@ -368,7 +382,9 @@ NqpuError   nqpu_batch_prepare(NqpuBatch* batch);
 /* Replay the graph; results[i] = <H> of circuit i (FP64).  len >= circuits. */
 NqpuError   nqpu_batch_run(NqpuBatch* batch, double* results, uint32_t len);
 /* out[0..4] = circuits, small circuits, tasks, HBM arena bytes, tiled passes;
- * out[5] (len >= 6) = bytes of tables uploaded host->device by prepare(). */
+ * out[5] (len >= 6) = bytes of tables uploaded host->device by prepare();
+ * out[6..9] (len >= 10) = host microseconds of the last prepare() in its
+ * phases: plans, table packing, device allocation and upload, graph capture. */
 NqpuError   nqpu_batch_stats(const NqpuBatch* batch, uint64_t* out, uint32_t len);
 /* Device time of the last run() (CUDA events around the graph replay on the
  * batch's stream: counter resets, the persistent launch, the result copy). */

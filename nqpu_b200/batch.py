@@ -43,6 +43,34 @@ class Batch:
         self.count += 1
         return int(idx.value)
 
+    def add_ising_arrays(self, items) -> int:
+        """Add many circuits in one nqpu_batch_add_ising_arrays call.  items:
+        (n, (codes [G], qubits [G, 3], params [G, 4]), J [n-1], h [n]) per
+        circuit, the gate arrays in the encoding of Circuit.from_arrays (no
+        custom-matrix gates).  Returns the index of the first circuit."""
+        items = list(items)
+        if not items:
+            return self.count
+        nq = np.array([it[0] for it in items], dtype=np.uint32)
+        counts = np.array([len(it[1][0]) for it in items], dtype=np.uint64)
+        offs = np.zeros(len(items) + 1, dtype=np.uint64)
+        np.cumsum(counts, out=offs[1:])
+        codes = np.ascontiguousarray(np.concatenate([np.asarray(it[1][0], dtype=np.uint32) for it in items]))
+        qubits = np.ascontiguousarray(np.concatenate([np.asarray(it[1][1], dtype=np.int32).reshape(-1, 3)
+                                                      for it in items]))
+        params = np.ascontiguousarray(np.concatenate([np.asarray(it[1][2], dtype=np.float64).reshape(-1, 4)
+                                                      for it in items]))
+        J = np.ascontiguousarray(np.concatenate([np.asarray(it[2], dtype=np.float64) for it in items]))
+        h = np.ascontiguousarray(np.concatenate([np.asarray(it[3], dtype=np.float64) for it in items]))
+        first = C.c_uint32()
+        check(self.lib.nqpu_batch_add_ising_arrays(
+            self.h_, len(items), nq.ctypes.data_as(C.POINTER(C.c_uint32)), offs.ctypes.data_as(C.POINTER(C.c_uint64)),
+            codes.ctypes.data_as(C.POINTER(C.c_uint32)), qubits.ctypes.data_as(C.POINTER(C.c_int32)),
+            params.ctypes.data_as(C.POINTER(C.c_double)), None, J.ctypes.data_as(C.POINTER(C.c_double)),
+            h.ctypes.data_as(C.POINTER(C.c_double)), C.byref(first)), "batch_add_arrays")
+        self.count += len(items)
+        return int(first.value)
+
     def config(self, **kw):
         for k, v in kw.items():
             check(self.lib.nqpu_batch_config(self.h_, PARAMS[k], int(v)), f"batch_config {k}")
@@ -62,10 +90,12 @@ class Batch:
         return float(ms.value)
 
     def stats(self) -> dict:
-        out = (C.c_uint64 * 6)()
-        check(self.lib.nqpu_batch_stats(self.h_, out, 6), "batch_stats")
+        out = (C.c_uint64 * 10)()
+        check(self.lib.nqpu_batch_stats(self.h_, out, 10), "batch_stats")
         return {"circuits": out[0], "small": out[1], "tasks": out[2], "arena_bytes": out[3], "passes": out[4],
-                "upload_bytes": out[5]}
+                "upload_bytes": out[5],
+                "prepare_s": {"plans": out[6] / 1e6, "pack": out[7] / 1e6, "alloc_upload": out[8] / 1e6,
+                              "capture": out[9] / 1e6}}
 
 
 def ising_terms(n, J, h):

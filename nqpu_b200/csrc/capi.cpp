@@ -590,12 +590,10 @@ extern "C" NqpuError nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uin
   return add_rec(c, g);
 }
 
-extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t* codes, const int32_t* qubits,
-                                            const double* params, const NqpuComplex* matrices, uint32_t count) {
-  if (!circuit) return NQPU_NULL_POINTER;
+NqpuError nqpu::circuit_append_gates(CircuitImpl* c, const uint32_t* codes, const int32_t* qubits,
+                                     const double* params, const NqpuComplex* matrices, size_t count) {
   if (count == 0) return NQPU_OK;
   if (!codes || !qubits || !params) return NQPU_NULL_POINTER;
-  CircuitImpl* c = Cc(circuit);
   // the records are written in place after the existing gates and dropped
   // again when any of them is rejected (the circuit is then unchanged)
   const size_t base = c->gates.size();
@@ -633,6 +631,12 @@ extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t
   }
   c->version++;
   return NQPU_OK;
+}
+
+extern "C" NqpuError nqpu_circuit_add_gates(NqpuCircuit* circuit, const uint32_t* codes, const int32_t* qubits,
+                                            const double* params, const NqpuComplex* matrices, uint32_t count) {
+  if (!circuit) return NQPU_NULL_POINTER;
+  return circuit_append_gates(Cc(circuit), codes, qubits, params, matrices, size_t(count));
 }
 
 static bool mode_ok(NqpuMode mode) {

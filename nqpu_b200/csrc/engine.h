@@ -81,6 +81,11 @@ struct Segment {
 };
 std::vector<Segment> circuit_segments(const std::vector<GateRec>& gates);
 bool circuit_has_mid(const std::vector<GateRec>& gates);
+// Append gates given as the flat arrays of nqpu_circuit_add_gates (each
+// checked as its single add would check it; nothing is appended unless all
+// are valid).  Defined with the C ABI (capi.cpp).
+NqpuError circuit_append_gates(CircuitImpl* c, const uint32_t* codes, const int32_t* qubits, const double* params,
+                               const NqpuComplex* matrices, size_t count);
 
 // Measure one qubit (collapse with the thread-local RNG draw, c_ffi.rs:537-560
 // rule) / project it onto |0> and renormalise (lib.rs:1705).

@@ -114,3 +114,14 @@ def test_plan_stats_brickwork():
     st12 = c.plan_stats(30, "c128", "tiled")
     assert st12["passes"] >= st13["passes"]
     assert lib.nqpu_tile_config_set(1, 3) == INVALID_PARAMETER
+
+
+def test_batch_bulk_add_rejects_without_a_device_call():
+    """Argument checks of nqpu_batch_add_ising_arrays that need no batch
+    handle: a NULL batch is NQPU_NULL_POINTER."""
+    import ctypes as C
+    from nqpu_b200 import _lib
+    lib = _lib.load()
+    nq = (C.c_uint32 * 1)(6)
+    offs = (C.c_uint64 * 2)(0, 0)
+    assert lib.nqpu_batch_add_ising_arrays(None, 1, nq, offs, None, None, None, None, None, None, None) == 5

@@ -74,3 +74,19 @@ def test_batch_configs_agree(cfg):
     base = make_batch(items).run()
     other = make_batch(items, **cfg).run()
     np.testing.assert_allclose(other, base, atol=1e-5, rtol=0)
+
+
+def test_bulk_add_from_arrays_is_bitwise_the_same():
+    """nqpu_batch_add_ising_arrays (every circuit's gate arrays in one call)
+    builds the same batch as one nqpu_batch_add_ising per circuit handle."""
+    items = workload(48, 21, 5, 16)
+    arrs = circuits.hea_batch(48, 21, nmin=5, nmax=16, lmin=2, lmax=6, arrays=True)
+    one = make_batch(items)
+    r1 = one.run()
+    one.close()
+    bulk = Batch()
+    assert bulk.add_ising_arrays(arrs[:20]) == 0
+    assert bulk.add_ising_arrays(arrs[20:]) == 20
+    r2 = bulk.run()
+    bulk.close()
+    assert np.array_equal(r1, r2)
