@@ -870,7 +870,8 @@ def run_serve(args):
     circs = [Circuit(r["n"], brickwork(r["n"], r["depth"], r["seed"])) for r in base]
     build_s = time.perf_counter() - t0
     G = sum(c.gate_count for c in circs)
-    pstats = [c.plan_stats(r["n"], "c64", "tiled") for c, r in zip(circs, base)]
+    # the server runs each request in NQPU_MODE_AUTO's choice (tensor-core or tiled passes)
+    pstats = [c.plan_stats(r["n"], "c64", "auto") for c, r in zip(circs, base)]
     passes = [p_["passes"] for p_ in pstats]
     # bytes each rate step moves: every request's plan tables (and its shot
     # uniforms) host->device, its <Z_i> or outcomes device->host
@@ -951,7 +952,7 @@ def run_serve(args):
             svc.append(time.perf_counter() - t)
             if r["n"] <= 26:
                 sv.reset()
-                c.execute(sv, "tiled")  # the server's computation (bitwise, tested)
+                c.execute(sv, "auto")  # the server's computation (bitwise, tested)
                 with StateVector(r["n"], "c128") as s128:
                     c.execute(s128, "tiled")
                     max_inf = max(max_inf, 1.0 - sv.fidelity(s128))

@@ -286,16 +286,19 @@ static bool plan_host(const CircuitImpl* c, const Segment& seg, uint32_t n, DTyp
 }
 
 // NQPU_MODE_AUTO: a device-time model in units of one HBM pass over the
-// state (2 S bytes; every cost below scales with 2^n, so the choice does not
-// depend on n).  Tiled passes: one unit per pass plus the shared-memory tile
-// work of each op (dense 1-qubit 0.15, dense 2-qubit 0.30, diagonal 0.058,
-// permutations free: they are deferred into the write-back addresses).
-// Tensor passes: one unit per pass plus 0.35 per fused unitary (its MMAs and
-// epilogue on every tile).  The coefficients are fits to 30-qubit complex64
-// runs of the brickwork (tiled 69 passes / 1200 U3, tensor 81 passes / 178
-// unitaries) and of the QFT (tiled 8 passes / 30 H + 435 controlled phases)
-// against the copy time of the state.  The tensor mode is taken when its
-// model is at least 10 % below the tiled one.
+// state (2 S bytes).  Tiled passes: per pass one unit plus its launch cost,
+// plus the shared-memory tile work of each op (dense 1-qubit 0.15, dense
+// 2-qubit 0.30, diagonal 0.058, permutations free: they are deferred into the
+// write-back addresses).  Tensor passes: per pass one unit plus its launch
+// cost, plus 0.35 per fused unitary (its MMAs and epilogue on every tile).
+// The launch cost is about 15 us per pass in either mode (launch, pass-table
+// prologue, grid tail), i.e. 15 us / (2 S / 6.5 TB/s) units: negligible at 30
+// qubits, dominant below 20, where the mode with fewer passes wins.  The
+// per-op coefficients are fits to 30-qubit complex64 runs of the brickwork
+// (tiled 69 passes / 1200 U3, tensor 81 passes / 178 unitaries) and of the
+// QFT (tiled 8 passes / 30 H + 435 controlled phases) against the copy time
+// of the state.  The tensor mode is taken when its model is at least 10 %
+// below the tiled one.
 int auto_mode_for(const std::vector<Op>& ops, uint32_t n, DType dt) {
   if (dt != DType::C64 || int(n) < kTcMinQubits) return NQPU_MODE_TILED;
   PlanStats ts;
@@ -314,8 +317,10 @@ int auto_mode_for(const std::vector<Op>& ops, uint32_t n, DType dt) {
       default: break;  // OP_X1, OP_SW
     }
   }
-  const double tiled = double(tp.stats.passes) + work;
-  const double tensor = double(ts.passes) + 0.35 * double(ts.stages);
+  const double pass_us = 2.0 * std::ldexp(8.0, int(n)) / 6.5e6;  // 2 S bytes at 6.5 TB/s, in microseconds
+  const double per_pass = 1.0 + 15.0 / pass_us;
+  const double tiled = double(tp.stats.passes) * per_pass + work;
+  const double tensor = double(ts.passes) * per_pass + 0.35 * double(ts.stages);
   return tensor < 0.9 * tiled ? NQPU_MODE_TENSOR : NQPU_MODE_TILED;
 }
 

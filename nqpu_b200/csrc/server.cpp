@@ -40,6 +40,7 @@
 #include "engine.h"
 #include "kernels.h"
 #include "planner.h"
+#include "tcrun.h"
 
 namespace nqpu {
 namespace {
@@ -110,6 +111,9 @@ struct Request {
   uint64_t seed = 0;
   bool tiled = false;
   TilePlan plan;
+  bool tensor = false;                 // tensor-core passes (NQPU_MODE_AUTO's choice)
+  TcPlan tcplan;
+  std::vector<size_t> bmat_off;        // B operands of each pass, in halves after off_stages
   std::vector<Op> ops;                 // per-gate path (states below the tiled minimum)
   std::vector<unsigned char> tables;   // passes | stages | ops, kTableAlign-aligned parts
   size_t off_stages = 0, off_ops = 0;
@@ -138,6 +142,9 @@ struct Lane {
   unsigned char* d_tab = nullptr;
   unsigned char* h_tab = nullptr;
   size_t tab_cap = 0;
+  double* d_tcnorm = nullptr;  // tensor passes: 3 x SM-count norm partials
+  int* d_tcerr = nullptr;      // tensor passes: bounded-wait expiry flag
+  int* h_tcerr = nullptr;
   std::vector<unsigned char*> old_h_tab;  // freed at shutdown
   std::shared_ptr<Request> req;
 };
@@ -184,7 +191,7 @@ cudaError_t launch_request(ServerImpl* sv, Lane& L, Request& r) {
   cudaStream_t st = L.stream;
   cudaError_t e;
   void* amp = sv->d_arena + r.mem_off;
-  if (r.tiled) {
+  if (r.tiled || r.tensor) {
     const size_t bytes = r.tables.size();
     if (bytes > L.tab_cap) {
       // grow the lane's table buffers: stream-ordered device free/alloc; the
@@ -203,7 +210,15 @@ cudaError_t launch_request(ServerImpl* sv, Lane& L, Request& r) {
     if ((e = cudaMemcpyAsync(L.d_tab, L.h_tab, bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
   }
   if ((e = launch_set_basis(DType::C64, amp, int(r.n), 0, st, sv->sms)) != cudaSuccess) return e;
-  if (r.tiled) {
+  if (r.tensor) {
+    if ((e = cudaMemsetAsync(L.d_tcerr, 0, sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = tc_launch(static_cast<float*>(amp), r.tcplan, reinterpret_cast<const TcPassRec*>(L.d_tab),
+                       reinterpret_cast<const uint16_t*>(L.d_tab + r.off_stages), r.bmat_off.data(), L.d_tcnorm,
+                       sv->sms, L.d_tcerr, st)) != cudaSuccess)
+      return e;
+    if ((e = cudaMemcpyAsync(L.h_tcerr, L.d_tcerr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return e;
+  } else if (r.tiled) {
     const PassRec* dp = reinterpret_cast<const PassRec*>(L.d_tab);
     const StageRec* ds = reinterpret_cast<const StageRec*>(L.d_tab + r.off_stages);
     const void* dops = L.d_tab + r.off_ops;
@@ -237,6 +252,7 @@ cudaError_t launch_request(ServerImpl* sv, Lane& L, Request& r) {
 void finish(ServerImpl* sv, Lane& L, cudaError_t result) {
   std::shared_ptr<Request> r = std::move(L.req);
   L.req.reset();
+  if (result == cudaSuccess && r->tensor && *L.h_tcerr) result = cudaErrorLaunchTimeout;  // a bounded wait expired
   if (result == cudaSuccess) {
     if (r->kind == NQPU_REQUEST_ZALL) {
       r->z.resize(r->n);
@@ -349,6 +365,9 @@ void server_free(ServerImpl* sv) {
     if (L.h_small) cudaFreeHost(L.h_small);
     if (L.h_uni) cudaFreeHost(L.h_uni);
     if (L.h_shots) cudaFreeHost(L.h_shots);
+    if (L.d_tcnorm) cudaFree(L.d_tcnorm);
+    if (L.d_tcerr) cudaFree(L.d_tcerr);
+    if (L.h_tcerr) cudaFreeHost(L.h_tcerr);
     if (L.h_tab) cudaFreeHost(L.h_tab);
     for (unsigned char* p : L.old_h_tab) cudaFreeHost(p);
     if (L.stream) cudaStreamDestroy(L.stream);
@@ -407,6 +426,10 @@ extern "C" NqpuServer* nqpu_server_create(const NqpuServerConfig* config) {
     ok = ok && cudaMallocHost(reinterpret_cast<void**>(&L.h_uni), c.max_shots * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc(reinterpret_cast<void**>(&L.d_shots), c.max_shots * sizeof(uint64_t)) == cudaSuccess;
     ok = ok && cudaMallocHost(reinterpret_cast<void**>(&L.h_shots), c.max_shots * sizeof(uint64_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(reinterpret_cast<void**>(&L.d_tcnorm), 3 * size_t(sv->sms) * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(reinterpret_cast<void**>(&L.d_tcerr), sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMallocHost(reinterpret_cast<void**>(&L.h_tcerr), sizeof(int)) == cudaSuccess;
+    if (ok) *L.h_tcerr = 0;
   }
   if (!ok) {
     cudaGetLastError();
@@ -448,7 +471,23 @@ extern "C" NqpuError nqpu_server_submit(NqpuServer* server, const NqpuCircuit* c
   r->seed = seed;
   r->large = c->n >= sv->cfg.large_qubits;
   std::vector<Op> ops = lower_circuit(c->gates);
-  if (int(c->n) >= tile_min_qubits(DType::C64)) {
+  if (auto_mode_for(ops, c->n, DType::C64) == NQPU_MODE_TENSOR) {
+    // the engine's own choice (NQPU_MODE_AUTO): tensor-core passes; tables =
+    // pass records | B operands
+    std::string err;
+    if (!build_tc_plan(ops, int(c->n), &r->tcplan, &err)) return NQPU_INVALID_PARAMETER;
+    r->tensor = true;
+    tc_bmat_offsets(r->tcplan, &r->bmat_off);
+    const size_t bp = r->tcplan.passes.size() * sizeof(TcPassRec);
+    const size_t bb = r->tcplan.bmats.size() * sizeof(uint16_t);
+    r->off_stages = align_up(bp);
+    r->tables.assign(r->off_stages + std::max<size_t>(bb, 1), 0);
+    if (bp) std::memcpy(r->tables.data(), r->tcplan.passes.data(), bp);
+    if (bb) std::memcpy(r->tables.data() + r->off_stages, r->tcplan.bmats.data(), bb);
+    r->tcplan.unitaries.clear();  // FP64 copies for tests only
+    r->tcplan.bmats.clear();
+    r->tcplan.bmats.shrink_to_fit();
+  } else if (int(c->n) >= tile_min_qubits(DType::C64)) {
     std::string err;
     if (!build_tile_plan(ops, int(c->n), DType::C64, tile_kmax_for(DType::C64), &r->plan, &err))
       return NQPU_INVALID_PARAMETER;

@@ -560,9 +560,9 @@ void tc_plan_free(void* plan) {
   delete p;
 }
 
-cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
-  auto* p = static_cast<TcPlanImpl*>(plan);
-  if (!p || s->dt != DType::C64 || int(s->n) != p->plan.n) return cudaErrorInvalidValue;
+cudaError_t tc_launch(float* amp, const TcPlan& plan, const TcPassRec* d_passes, const uint16_t* d_bmats,
+                      const size_t* bmat_off, double* d_norm, int slots, int* d_err, cudaStream_t st,
+                      std::vector<cudaEvent_t>* events) {
   static PerDeviceOnce<cudaError_t> attr;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -570,25 +570,41 @@ cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
   e = attr.get(dev, [] { return cudaFuncSetAttribute(k_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)); },
                cudaErrorInvalidDevice);
   if (e != cudaSuccess) return e;
-  const uint32_t n_tiles = uint32_t(1) << (p->plan.n - kTcTileBits);
+  const uint32_t n_tiles = uint32_t(1) << (plan.n - kTcTileBits);
   const unsigned grid =
-      unsigned(std::min<uint64_t>((uint64_t(n_tiles) + kTcEngines - 1) / kTcEngines, uint64_t(p->slots)));
-  double* norm0 = p->d_norm;
-  for (size_t i = 0; i < p->plan.passes.size(); ++i) {
-    double* outn = p->d_norm + (1 + (i & 1)) * size_t(p->slots);
-    const double* prevn = i ? p->d_norm + (1 + ((i + 1) & 1)) * size_t(p->slots) : nullptr;
-    k_tc_pass<<<grid, kTcThreads, kTcSmem, s->stream>>>(
-        static_cast<float*>(s->amp), p->d_passes + i, p->d_bmats + p->bmat_off[i], n_tiles, p->plan.state_scale,
-        i ? norm0 : nullptr, i ? nullptr : norm0, prevn, int(grid), outn, p->d_err);
+      unsigned(std::min<uint64_t>((uint64_t(n_tiles) + kTcEngines - 1) / kTcEngines, uint64_t(slots)));
+  double* norm0 = d_norm;
+  for (size_t i = 0; i < plan.passes.size(); ++i) {
+    double* outn = d_norm + (1 + (i & 1)) * size_t(slots);
+    const double* prevn = i ? d_norm + (1 + ((i + 1) & 1)) * size_t(slots) : nullptr;
+    k_tc_pass<<<grid, kTcThreads, kTcSmem, st>>>(amp, d_passes + i, d_bmats + bmat_off[i], n_tiles, plan.state_scale,
+                                                  i ? norm0 : nullptr, i ? nullptr : norm0, prevn, int(grid), outn,
+                                                  d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (events) {
       cudaEvent_t ev;
       if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
       events->push_back(ev);
-      if ((e = cudaEventRecord(ev, s->stream)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(ev, st)) != cudaSuccess) return e;
     }
   }
   return cudaSuccess;
+}
+
+void tc_bmat_offsets(const TcPlan& plan, std::vector<size_t>* off) {
+  off->clear();
+  size_t o = 0;
+  for (const TcPassRec& P : plan.passes) {
+    off->push_back(o);
+    o += size_t(P.m) * kTcBmatHalves;
+  }
+}
+
+cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
+  auto* p = static_cast<TcPlanImpl*>(plan);
+  if (!p || s->dt != DType::C64 || int(s->n) != p->plan.n) return cudaErrorInvalidValue;
+  return tc_launch(static_cast<float*>(s->amp), p->plan, p->d_passes, p->d_bmats, p->bmat_off.data(), p->d_norm,
+                   p->slots, p->d_err, s->stream, events);
 }
 
 cudaError_t tc_check_error(void* plan, cudaStream_t st) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <vector>
 #include "sv_types.h"
+#include "tcpass.h"
 
 namespace nqpu {
 struct StateImpl;
@@ -14,4 +15,13 @@ void tc_plan_free(void* plan);
 cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events);
 // Reads the plan's device error flag (set when a bounded wait expired).
 cudaError_t tc_check_error(void* plan, cudaStream_t st);
+// Queue the passes of a host plan whose records and B operands are already in
+// device memory: pass i's record at d_passes + i, its B operands at d_bmats +
+// bmat_off[i] (tc_bmat_offsets); d_norm holds 3 * slots doubles of scratch
+// (the grid is at most `slots` CTAs), *d_err is set when a bounded wait
+// expires.  With `events`, an event is recorded after every launch.
+cudaError_t tc_launch(float* amp, const TcPlan& plan, const TcPassRec* d_passes, const uint16_t* d_bmats,
+                      const size_t* bmat_off, double* d_norm, int slots, int* d_err, cudaStream_t st,
+                      std::vector<cudaEvent_t>* events = nullptr);
+void tc_bmat_offsets(const TcPlan& plan, std::vector<size_t>* off);
 }  // namespace nqpu

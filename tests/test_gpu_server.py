@@ -2,9 +2,10 @@
 circuits on device-resident complex64 states).
 
 Tolerance: each request's result is bitwise the same whether it runs alone or
-in a mix, and bitwise the same as the state API's tiled path (same plan, same
-kernels, same launch shapes, same seeded uniforms); against the FP64 oracle,
-max |d<Z_i>| <= 1e-5 (the complex64 bar)."""
+in a mix, and bitwise the same as the state API run in NQPU_MODE_AUTO (the
+server makes the same engine choice: same plan, same kernels, same launch
+shapes, same seeded uniforms); against the FP64 oracle, max |d<Z_i>| <= 1e-5
+(the complex64 bar)."""
 import numpy as np
 import pytest
 
@@ -50,7 +51,7 @@ def test_results_same_alone_in_mix_and_as_state_api():
             alone = run_all(solo, [r])[0]
         assert np.array_equal(alone, got), r
         with StateVector(r["n"], "c64") as sv:
-            Circuit(r["n"], r["gates"]).execute(sv, "tiled")
+            Circuit(r["n"], r["gates"]).execute(sv, "auto")
             if r["kind"] == "zall":
                 ref = sv.expectation_z_all()
             else:

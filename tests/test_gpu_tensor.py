@@ -142,7 +142,7 @@ def test_rejects_complex128_and_small_states():
         c.execute(sv, "tensor")
 
 
-@pytest.mark.parametrize("n,kind,dtype", [(20, "brickwork", "c64"), (20, "qft", "c64"), (16, "tfim", "c64"),
+@pytest.mark.parametrize("n,kind,dtype", [(22, "brickwork", "c64"), (20, "qft", "c64"), (16, "tfim", "c64"),
                                           (18, "brickwork", "c128"), (10, "brickwork", "c64")])
 def test_auto_mode_matches_oracle(n, kind, dtype):
     """NQPU_MODE_AUTO runs each gate run in the mode its model picks; the
