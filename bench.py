@@ -191,6 +191,7 @@ def run_reference(args):
 # per pass), so the per-launch traffic is this figure times 2^n.
 DRAM_BYTES_PER_AMP = {
     "k_tile_pass": 15.14,  # 26q brickwork depth 8, two launches averaged
+    "k_tc_pass": 15.19,    # 26q brickwork depth 10, two launches (537.0 MB read + 482.6 MB written each)
 }
 
 
@@ -314,7 +315,8 @@ def run_engine(args):
     traffic = traffic_per_launch(kernel, n) if args.dtype == "c64" else None
     roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": traffic, "algorithmic_bytes_per_launch": 2 * S,
+                "traffic": traffic, "traffic_source": "ncu DRAM bytes per amplitude of a 26-qubit capture x 2^n",
+                "algorithmic_bytes_per_launch": 2 * S,
                 "launches_per_step": stats["passes"], "avg_launch_ms": avg_launch_ms,
                 "pass_time_share": (sum(launch_ms) / el_ms) if el_ms else None}
     mhz = (clk or {}).get("sm_mhz") or 1965.0

@@ -285,7 +285,10 @@ static bool plan_host(const CircuitImpl* c, const Segment& seg, uint32_t n, DTyp
   return true;
 }
 
-// NQPU_MODE_AUTO: a device-time model in units of one HBM pass over the
+// NQPU_MODE_AUTO: the engine mode with the lower modelled device time (the
+// counterpart of the reference's runtime-estimate backend choice,
+// select_backend_estimated, backends/runtime/auto_simulator.rs:1452, among
+// its statevector variants).  The model is in units of one HBM pass over the
 // state (2 S bytes).  Tiled passes: per pass one unit plus its launch cost,
 // plus the shared-memory tile work of each op (dense 1-qubit 0.15, dense
 // 2-qubit 0.30, diagonal 0.058, permutations free: they are deferred into the
