@@ -16,15 +16,15 @@
 //            power of two, for the FP16 range) and the renormalisation
 //            factor, splits x = hi + lo into FP16 pairs and stores them in
 //            unitary 0's operand layout;
-//   unitary  one elected thread issues 8 MMAs (K = 16): D[:, 0:128] =
-//            A_hi [B_hi; B_lo]^T (N = 128) then D[:, 0:64] += A_lo B_hi^T
-//            (N = 64), B = the real embedding of 16 U, and commits them to
+//   unitary  one elected thread issues 12 MMAs (K = 16, N = 64) into the
+//            engine's 64-column accumulator: D = A_hi B_hi^T + A_hi B_lo^T +
+//            A_lo B_hi^T, B = the real embedding of 16 U, and commits them to
 //            the engine's mbarrier; one warp polls it (bounded) while the
 //            other three wait at the engine's named barrier;
-//   epilogue each thread drains its row (TMEM lane) of D, two 4-column parts
-//            per TMEM load wait, forms out = (D[:, 0:64] + D[:, 64:128]) / 16
-//            and either splits it straight into the next unitary's operand
-//            layout, or, after the last unitary, stores out / s to HBM.
+//   epilogue each thread drains its row (TMEM lane) of D, four 4-column
+//            parts per TMEM load wait, forms out = D / 16 and either splits
+//            it straight into the next unitary's operand layout, or, after
+//            the last unitary, stores out / s to HBM.
 // While one engine waits for its MMAs the other three run, so the tensor
 // pipe, shared memory and HBM overlap across four tiles.  The B operands of
 // the pass's unitaries stay in shared memory for the launch.
@@ -66,13 +66,20 @@ constexpr int kTcLoadSteps = 1 << kTcStpBits;                 // 16-byte chunks 
 constexpr int kTcColHalves = kTcEngineWarps / 4;              // warps sharing a lane quadrant
 constexpr int kTcCols = 32 / kTcColHalves;                    // complex columns a thread drains
 constexpr int kTcParts = kTcCols / 4;                         // epilogue parts of 4 columns
-constexpr int kTcBatch = 2;                                   // parts per TMEM load wait (4: spills)
+// All three split products accumulate into one 64-column accumulator (12
+// MMAs of N = 64).  (Measured against A_hi [B_hi; B_lo]^T with N = 128 plus
+// A_lo B_hi^T into 128 columns summed in the epilogue: the same speed, half
+// the infidelity, half the TMEM loads; a fifth engine, which the 64-column
+// accumulators would allow, measured 1.5 % slower at 96 registers.)
+constexpr int kTcBatch = 4;                                   // parts per TMEM load wait
+constexpr uint32_t kTcAccCols = 64;                           // accumulator columns per engine
+static_assert(kTcEngines * kTcAccCols <= 512, "accumulators fit tensor memory");
 static_assert(kTcParts % kTcBatch == 0, "whole batches");
 constexpr uint32_t kTcAPlane = 128 * 128;            // 16 KB: 128 rows x 64 halves
 constexpr uint32_t kTcOpBytes = 2 * kTcAPlane;       // hi + lo planes
 constexpr uint32_t kTcBBytes = 128 * 128;            // [B_hi; B_lo]: 128 rows x 64 halves
 constexpr uint32_t kTcWaitLimit = 1u << 22;          // bounded mbarrier polls
-constexpr uint32_t kTcTmemCols = 512;                // four engines x one 128-column accumulator
+constexpr uint32_t kTcTmemCols = 512;                // the engines' accumulators (allocated as a power of two)
 
 // Every offset the kernel forms is GF(2)-linear in the bits of its index (the
 // swizzled operand layout XORs disjoint fields; amplitude offsets OR disjoint
@@ -89,7 +96,6 @@ constexpr size_t kTcSmem = 1024 /*alignment*/ + kTcEngines * size_t(kTcOpBytes) 
                            kTcMaxUnitaries * size_t(kTcBBytes) + sizeof(TcTables);
 static_assert(kTcSmem <= 232448, "dynamic shared memory of one CTA");
 
-constexpr uint32_t kIdescN128 = umma_idesc_f16<128, 128>();
 constexpr uint32_t kIdescN64 = umma_idesc_f16<128, 64>();
 
 __device__ __forceinline__ void engine_sync(int e) {
@@ -246,7 +252,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t alo_s = ahi_s + kTcAPlane;
   const uint32_t b_s = static_cast<uint32_t>(__cvta_generic_to_shared(bbuf));
   const uint32_t my_mbar = mbar_s + 8u * uint32_t(e);
-  const uint32_t acc = tmem + 128u * uint32_t(e);
+  const uint32_t acc = tmem + kTcAccCols * uint32_t(e);
   const uint32_t lanes = acc + (uint32_t(q * 32) << 16) + uint32_t(2 * kTcCols * ch);
 
   auto tile_base_of = [&](uint32_t tile) {
@@ -342,7 +348,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint64_t dhi = umma_desc_sw128(ahi_s), dlo = umma_desc_sw128(alo_s);
         const uint64_t dbj = umma_desc_sw128(b_s + uint32_t(j) * kTcBBytes);
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dhi + 2u * kk, dbj + 2u * kk, kIdescN128, kk > 0 ? 1u : 0u);
+        // D = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T; B_lo = rows 64..127 of
+        // the B buffer: 8 KB on, a whole number of 1 KB swizzle atoms (512 in
+        // the descriptor's 16-byte units)
+        for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dhi + 2u * kk, dbj + 2u * kk, kIdescN64, kk > 0 ? 1u : 0u);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dhi + 2u * kk, dbj + 512u + 2u * kk, kIdescN64, 1u);
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) umma_f16(acc, dlo + 2u * kk, dbj + 2u * kk, kIdescN64, 1u);
         umma_commit(my_mbar);
@@ -408,12 +419,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const float2 sc = make_float2(scv, scv);
 #pragma unroll
       for (int pb = 0; pb < kTcParts; pb += kTcBatch) {
-        uint32_t rh[kTcBatch][8], rl[kTcBatch][8];
+        uint32_t rh[kTcBatch][8];
 #pragma unroll
-        for (int k = 0; k < kTcBatch; ++k) {
-          tmem_ld8(lanes + 8u * uint32_t(pb + k), rh[k]);
-          tmem_ld8(lanes + 64u + 8u * uint32_t(pb + k), rl[k]);
-        }
+        for (int k = 0; k < kTcBatch; ++k) tmem_ld8(lanes + 8u * uint32_t(pb + k), rh[k]);
         tmem_ld_wait();
 #pragma unroll
         for (int k = 0; k < kTcBatch; ++k) {
@@ -428,13 +436,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 xo ^= xb[b];
                 go += gb[b];
               }
-            // out = (D[:, 0:64] + D[:, 64:128]) * scale, packed (re, im)
-            const float2 x0 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[k][2 * cc]), __uint_as_float(rh[k][2 * cc + 1])),
-                                                    make_float2(__uint_as_float(rl[k][2 * cc]), __uint_as_float(rl[k][2 * cc + 1]))),
-                                         sc);
-            const float2 x1 = __fmul2_rn(__fadd2_rn(make_float2(__uint_as_float(rh[k][2 * cc + 2]), __uint_as_float(rh[k][2 * cc + 3])),
-                                                    make_float2(__uint_as_float(rl[k][2 * cc + 2]), __uint_as_float(rl[k][2 * cc + 3]))),
-                                         sc);
+            // out = D * scale, packed (re, im)
+            const float2 x0 = __fmul2_rn(make_float2(__uint_as_float(rh[k][2 * cc]), __uint_as_float(rh[k][2 * cc + 1])), sc);
+            const float2 x1 =
+                __fmul2_rn(make_float2(__uint_as_float(rh[k][2 * cc + 2]), __uint_as_float(rh[k][2 * cc + 3])), sc);
             if (!last) {
               const uint32_t o0 = xbase ^ xo;
               if (my_pair) {
