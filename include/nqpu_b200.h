@@ -240,9 +240,8 @@ NqpuError    nqpu_circuit_add_custom_1q(NqpuCircuit* c, uint32_t q, const NqpuCo
 NqpuError    nqpu_circuit_add_custom_2q(NqpuCircuit* c, uint32_t q1, uint32_t q2, const NqpuComplex* matrix);
 /* No counterpart in the reference.  All <Z_i> (FP64) of a state that lives in
  * the CALLER's device memory, for callers that cannot allocate device memory:
- * plugins whose host runtime owns the device memory pool, real-time loops that
- * must not wait on the allocator, code running while its stream is captured
- * (where cudaMalloc is not permitted).  It allocates nothing: the reduction's
+ * plugins whose host runtime owns the device memory pool, and real-time loops
+ * that must not wait on the allocator.  It allocates nothing: the reduction's
  * scratch is a fixed array in this library's device module (about 2.2 MB on
  * every GPU that loads the library, kept until exit).  d_amplitudes: 2^n
  * interleaved (re, im) amplitudes of `dtype`, 16-byte aligned; d_out: n doubles

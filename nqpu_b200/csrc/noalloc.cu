@@ -3,9 +3,8 @@
 // Some callers of this library cannot call cudaMalloc themselves or through
 // us: plugins hosted inside another runtime that owns the device memory pool
 // (its allocator must be the only one, or memory it has reserved would be
-// taken from under it), real-time loops that must not block on the driver's
-// allocator, and code that runs while its stream is being captured, where
-// cudaMalloc is not permitted.  nqpu_expectation_z_all_noalloc serves them:
+// taken from under it), and real-time loops that must not block on the
+// driver's allocator.  nqpu_expectation_z_all_noalloc serves them:
 // the caller passes its own device amplitude buffer, its own device output
 // buffer and its stream, and the reduction's scratch space comes from a fixed
 // array in device global memory that is part of this library's module (loaded

@@ -1,9 +1,8 @@
 """The no-allocation all-<Z_i> entry point against the regular one.
 
 nqpu_expectation_z_all_noalloc is for callers that cannot allocate device
-memory: plugins whose host runtime owns the device memory pool, real-time loops
-that must not wait on the allocator, code running while its stream is captured
-(where cudaMalloc is not permitted).  The caller owns the amplitude and output
+memory: plugins whose host runtime owns the device memory pool, and real-time
+loops that must not wait on the allocator.  The caller owns the amplitude and output
 buffers; the entry point takes its scratch from a fixed device array of the
 library, so its size is capped (complex64 up to 28 qubits, complex128 up to 27)
 and the cases at those caps fill the array.  This file is collected last so
