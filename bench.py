@@ -806,8 +806,6 @@ def run_batch(args):
                "timing": "host wall clock: batch from the circuits' gate arrays (one nqpu_batch_add_ising_arrays "
                          "call), prepare (plans on host threads, uploads, graph capture), one replay, results on the host"}
         b2.close()
-        for c in cs:
-            c.close()
 
     cpu = None
     if not args.quick and not args.no_cpu:
