@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (tid < 5 * m) {
     const int j = tid / 5, i = tid % 5;
     T->xcb[j][i] = j + 1 < m ? P.u[j + 1].boff[P.u[j].fcol[i]] : 0u;
-    T->gcb[j][i] = 1ull << P.qt[P.u[j].fcol[i]];
+    T->gcb[j][i] = 1ull << P.qt_out[P.u[j].fcol[i]];
   }
   if (tid < kTcStpBits) {
     T->sob[tid] = P.u[0].boff[P.lt[kTcThrBits + tid]];
@@ -243,10 +243,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       pair[j] = P.u[j + 1].boff[P.u[j].fcol[0]] == 4u;
     } else if (j + 1 == m) {
       for (int i = 0; i < 7; ++i)
-        if ((row >> i) & 1u) pg |= 1ull << P.qt[P.u[j].frow[i]];
+        if ((row >> i) & 1u) pg |= 1ull << P.qt_out[P.u[j].frow[i]];
     }
   }
-  const bool store16 = P.qt[P.u[m - 1].fcol[0]] == 0;  // qubit 0 is column bit 0 of the last layout
+  const bool store16 = P.qt_out[P.u[m - 1].fcol[0]] == 0;  // index bit 0 is column bit 0 of the last layout
 
   const uint32_t ahi_s = static_cast<uint32_t>(__cvta_generic_to_shared(opbuf)) + uint32_t(e) * kTcOpBytes;
   const uint32_t alo_s = ahi_s + kTcAPlane;

@@ -16,6 +16,7 @@
 // between unitaries: the epilogue of unitary j writes each amplitude straight
 // to its place in unitary j+1's operand.
 #pragma once
+#include <array>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -54,7 +55,9 @@ struct TcUnitaryRec {
 
 struct TcPassRec {
   int32_t m;                     // unitaries in this pass (1..kTcMaxUnitaries)
-  int32_t qt[kTcTileBits];       // qubit of tile bit b
+  int32_t qt[kTcTileBits];       // state index bit of tile bit b when the pass loads (0..4: bits 0..4)
+  int32_t qt_out[kTcTileBits];   // state index bit of tile bit b when the pass stores (a permutation
+                                 // of qt: the pass may move qubits between index bits, see TcPlan)
   int32_t n_out;                 // qubits outside Q (tile-id bits)
   int32_t qout[kMaxQubits];      // qubit of tile-id bit j, ascending
   // loader: tile bit of loading-thread bit b (b < kTcLoadThreadBits; bits 0..2
@@ -64,6 +67,13 @@ struct TcPassRec {
   TcUnitaryRec u[kTcMaxUnitaries];
 };
 
+// Qubit placement: a pass may store its tile with its qubits on other state
+// index bits than it loaded them from (qt_out), so that the qubits the next
+// pass needs sit on index bits 0..4, which every tile must contain (they make
+// the 256-byte runs of its HBM accesses).  Placements are swaps of a qubit on
+// bits 0..4 with one elsewhere; the plan's last pass (or an added pass with an
+// identity unitary) puts every qubit back on its own bit, so a run ends in
+// the natural order.
 struct TcPlan {
   int n = 0;
   float state_scale = 1.0f;      // amplitudes enter the operands multiplied by this power of two
@@ -75,6 +85,8 @@ struct TcPlan {
   // per pass, per unitary: the fused 32x32 complex unitary in FP64 (column index
   // = fcol bits), for the CPU emulator and tests
   std::vector<std::vector<cplx>> unitaries;
+  // per pass: the qubit of each tile bit (the ops' qubit numbering)
+  std::vector<std::array<int32_t, kTcTileBits>> lq;
   PlanStats stats;
 };
 

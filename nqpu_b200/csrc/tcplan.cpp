@@ -117,9 +117,9 @@ int layout_cost(const LayoutCfg& c, int m, const int* qt) {
   // minimum is 8 for 8-byte stores and 16 for 16-byte ones (qubit 0 is then a
   // column bit and each lane writes a pair).
   const int L = m - 1;
-  const bool wide = qt[c.fcol[L][0]] == 0;
+  const bool wide = qt[c.fcol[L][0]] == 0;  // qt: the store-side index bits (qt_out)
   int k = 0;
-  for (int i = 0; i < 5; ++i) k += (c.frow[L][i] == 0 || c.frow[L][i] == 1) ? 1 : 0;
+  for (int i = 0; i < 5; ++i) k += qt[c.frow[L][i]] <= 1 ? 1 : 0;  // the row bit stores to index bit 0 or 1
   const int ns = 32 >> k, ideal = wide ? 16 : 8;
   cost += (4 * (wide ? 16 : 32) * (ns - ideal)) / 4;
   return cost;
@@ -173,12 +173,12 @@ void choose_layouts(TcPassRec& P) {
     return int(rng % uint64_t(k));
   };
   auto descend = [&](LayoutCfg& c) {
-    int cc = layout_cost(c, m, P.qt);
+    int cc = layout_cost(c, m, P.qt_out);
     for (int iter = 0; iter < 64; ++iter) {
       int best = cc;
       LayoutCfg bc = c;
       auto consider = [&](const LayoutCfg& t) {
-        const int v = layout_cost(t, m, P.qt);
+        const int v = layout_cost(t, m, P.qt_out);
         if (v < best) {
           best = v;
           bc = t;
@@ -286,18 +286,33 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
   out->passes.clear();
   out->bmats.clear();
   out->unitaries.clear();
+  out->lq.clear();
   out->stats = PlanStats{};
   if (n < kTcMinQubits || n > kMaxQubits) {
     if (err) *err = "the tensor-core pass mode needs 12 <= n <= 34 qubits";
     return false;
   }
-  const uint64_t low = (1ull << kTcLowBits) - 1;
   std::vector<std::vector<int>> cluster_ops;  // ops of each unitary, in pass order
   std::vector<int> remaining(ops.size());
   for (size_t i = 0; i < ops.size(); ++i) remaining[i] = int(i);
-  while (!remaining.empty()) {
-    // ---- ops of the pass ----
-    uint64_t Q = low, blocked = 0;
+  // qubit placement: at[p] = qubit on state index bit p, pos[q] = index bit of
+  // qubit q.  Invariant: every displaced qubit is one of a swap pair (l, X),
+  // l < 5 <= X: qubit X on bit l and qubit l on bit X.
+  std::vector<int> at(static_cast<size_t>(n)), pos(static_cast<size_t>(n));
+  for (int q = 0; q < n; ++q) at[size_t(q)] = pos[size_t(q)] = q;
+  auto low_qubits = [&]() {
+    uint64_t m_ = 0;
+    for (int l = 0; l < kTcLowBits; ++l) m_ |= 1ull << at[size_t(l)];
+    return m_;
+  };
+  auto placed_home = [&]() {
+    for (int l = 0; l < kTcLowBits; ++l)
+      if (at[size_t(l)] != l) return false;
+    return true;
+  };
+  while (!remaining.empty() || !placed_home()) {
+    // ---- ops of the pass (the qubits on bits 0..4 are always in the tile) ----
+    uint64_t Q = low_qubits(), blocked = 0;
     std::vector<int> taken, rest;
     for (int idx : remaining) {
       const uint64_t qm = ops[size_t(idx)].qubit_mask();
@@ -347,33 +362,116 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
       std::merge(pend.begin(), pend.end(), rest.begin(), rest.end(), std::back_inserter(merged));
       rest.swap(merged);
     }
-    // fill the tile to 12 qubits with the lowest unused qubits
+    if (clusters.empty()) clusters.emplace_back(0, std::vector<int>());  // a placement-only pass: identity
+    // ---- the qubits the next pass wants on bits 0..4: the first qubits of
+    // the ops still to come (none left: the displaced low qubits, to go home) ----
+    std::vector<int> want;
+    {
+      uint64_t seen = 0;
+      for (int idx : rest) {
+        uint64_t qm = ops[size_t(idx)].qubit_mask() & ~seen;
+        while (qm && want.size() < size_t(kTcTileBits)) {
+          const int q = __builtin_ctzll(qm);
+          qm &= qm - 1;
+          seen |= 1ull << q;
+          want.push_back(q);
+        }
+        if (want.size() >= size_t(kTcTileBits)) break;
+      }
+      if (rest.empty())
+        for (int l = 0; l < kTcLowBits; ++l)
+          if (at[size_t(l)] != l) want.push_back(l);
+    }
+    // fill the tile to 12 qubits: wanted qubits first (they can then be
+    // placed on bits 0..4 by this pass's stores), then the lowest unused
+    for (int q : want)
+      if (popc(Q) < kTcTileBits) Q |= 1ull << q;
     for (int q = 0; q < n && popc(Q) < kTcTileBits; ++q) Q |= 1ull << q;
+    // ---- placement after the pass: wanted qubits onto bits 0..4 by swaps
+    // inside the tile (the tile's index bits are pos[Q]) ----
+    std::vector<int> at_new = at, pos_new = pos;
+    {
+      auto in_tile = [&](int q) { return ((Q >> q) & 1ull) != 0; };
+      // at most 5 wanted qubits that are in the tile, in order of need
+      std::vector<int> cand;
+      for (int q : want)
+        if (in_tile(q) && cand.size() < size_t(kTcLowBits)) cand.push_back(q);
+      auto is_cand = [&](int q) { return std::find(cand.begin(), cand.end(), q) != cand.end(); };
+      bool fixed[kTcLowBits] = {false, false, false, false, false};
+      for (int l = 0; l < kTcLowBits; ++l)
+        if (is_cand(at_new[size_t(l)])) fixed[l] = true;  // already where it is wanted
+      for (int y : cand) {
+        if (pos_new[size_t(y)] < kTcLowBits) continue;  // already on bits 0..4
+        if (y < kTcLowBits) {
+          // a low qubit displaced to bit X: swap it home if bit y is free to change
+          if (fixed[y]) continue;
+          const int x = at_new[size_t(y)];  // the qubit on bit y, whose home bit holds y
+          if (!in_tile(x)) continue;
+          at_new[size_t(y)] = y;
+          pos_new[size_t(y)] = y;
+          at_new[size_t(x)] = x;
+          pos_new[size_t(x)] = x;
+          fixed[y] = true;
+          continue;
+        }
+        // y >= 5 sits on its own bit y (the invariant): pick a low bit l to swap with
+        int best = -1;
+        for (int l = 0; l < kTcLowBits && best < 0; ++l)
+          if (!fixed[l] && at_new[size_t(l)] == l) best = l;  // bit l holds qubit l: a fresh pair
+        for (int l = 0; l < kTcLowBits && best < 0; ++l)
+          if (!fixed[l] && at_new[size_t(l)] != l && in_tile(l)) best = l;  // end the pair on bit l first
+        if (best < 0) continue;
+        const int l = best;
+        if (at_new[size_t(l)] != l) {
+          const int x = at_new[size_t(l)];  // qubit x on bit l, qubit l on bit x: x goes home
+          at_new[size_t(x)] = x;
+          pos_new[size_t(x)] = x;
+          at_new[size_t(l)] = l;
+          pos_new[size_t(l)] = l;
+        }
+        at_new[size_t(l)] = y;
+        pos_new[size_t(y)] = l;
+        at_new[size_t(y)] = l;
+        pos_new[size_t(l)] = y;
+        fixed[l] = true;
+      }
+    }
 
     TcPassRec P;
     std::memset(&P, 0, sizeof(P));
     P.m = int(clusters.size());
+    std::array<int32_t, kTcTileBits> lq{};
     {
+      // tile bits in the order of their index bits when loaded (bits 0..4
+      // first: the 256-byte runs); the stores use the new placement
       int b = 0;
-      for (int q = 0; q < n; ++q)
-        if ((Q >> q) & 1ull) P.qt[b++] = q;
+      for (int p = 0; p < n; ++p)
+        if ((Q >> at[size_t(p)]) & 1ull) {
+          lq[size_t(b)] = at[size_t(p)];
+          P.qt[b] = p;
+          P.qt_out[b] = pos_new[size_t(at[size_t(p)])];
+          ++b;
+        }
       int o = 0;
-      for (int q = 0; q < n; ++q)
-        if (!((Q >> q) & 1ull)) P.qout[o++] = q;
+      for (int p = 0; p < n; ++p)
+        if (!((Q >> at[size_t(p)]) & 1ull)) P.qout[o++] = p;
       P.n_out = o;
     }
     for (int j = 0; j < P.m; ++j) {
       uint64_t F = clusters[size_t(j)].first;
       // pad to exactly 5 qubits with the lowest unused tile qubits
-      for (int b = 0; b < kTcTileBits && popc(F) < 5; ++b) F |= 1ull << P.qt[b];
+      for (int b = 0; b < kTcTileBits && popc(F) < 5; ++b) F |= 1ull << lq[size_t(b)];
       int i = 0;
       for (int b = 0; b < kTcTileBits; ++b)
-        if ((F >> P.qt[b]) & 1ull) P.u[j].fcol[i++] = b;
+        if ((F >> lq[size_t(b)]) & 1ull) P.u[j].fcol[i++] = b;
     }
     out->passes.push_back(P);
+    out->lq.push_back(lq);
     for (auto& cl : clusters) cluster_ops.push_back(std::move(cl.second));
     out->stats.stages += uint64_t(P.m);
     remaining.swap(rest);
+    at.swap(at_new);
+    pos.swap(pos_new);
   }
   if (!finish) {
     out->stats.passes = out->passes.size();
@@ -400,7 +498,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
         for (int i = 0; i < 5; ++i)
           if ((c >> i) & 1u) {
             if (j + 1 < P.m) x ^= P.u[j + 1].boff[U.fcol[i]];
-            g |= 1ull << P.qt[U.fcol[i]];
+            g |= 1ull << P.qt_out[U.fcol[i]];
           }
         U.xnext[c] = x;
         U.gcol[c] = g;
@@ -409,7 +507,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     for (int j = 0; j < P.m; ++j) {
       const size_t ui = first_u[pi] + size_t(j);
       int q[5];
-      for (int i = 0; i < 5; ++i) q[i] = P.qt[P.u[j].fcol[i]];
+      for (int i = 0; i < 5; ++i) q[i] = out->lq[pi][size_t(P.u[j].fcol[i])];
       std::vector<cplx> u(32 * 32, cplx(0, 0));
       for (int c = 0; c < 32; ++c) {
         cplx col[32];

@@ -136,13 +136,13 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
         for (int i = 0; i < 5; ++i)
           if ((c >> i) & 1u) {
             if (j + 1 < m) x ^= P.u[j + 1].boff[P.u[j].fcol[i]];
-            g += 1ull << P.qt[P.u[j].fcol[i]];
+            g += 1ull << P.qt_out[P.u[j].fcol[i]];
           }
         if ((j + 1 < m && P.u[j].xnext[c] != x) || (j + 1 == m && P.u[j].gcol[c] != g)) return -4;
       }
     const uint32_t boff_h = P.u[0].boff[0];
     const bool load_pair = boff_h == 4u;  // tile bit 0 is column bit 0 of unitary 0
-    const bool store16 = P.qt[P.u[m - 1].fcol[0]] == 0;
+    const bool store16 = P.qt_out[P.u[m - 1].fcol[0]] == 0;
     std::vector<int> amp_written(dim, 0);
     for (uint64_t tile = 0; tile < n_tiles; ++tile) {
       uint64_t tb = 0;
@@ -192,7 +192,7 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
           for (int i = 0; i < 7; ++i)
             if ((r >> i) & 1u) {
               if (!last) ptn ^= P.u[j + 1].boff[P.u[j].frow[i]];
-              else pg |= 1ull << P.qt[P.u[j].frow[i]];
+              else pg |= 1ull << P.qt_out[P.u[j].frow[i]];
             }
           const bool pair = !last && P.u[j + 1].boff[P.u[j].fcol[0]] == 4u;
           for (uint32_t c = 0; c < 32; ++c) {
