@@ -2,7 +2,8 @@
 lib.rs:1835; GateOperations::reset_qubit, lib.rs:1705) against the oracle: with
 the same seed the engine and the oracle draw the same xorshift64* uniforms,
 so the outcomes must agree exactly and the final states within the dtype's
-tolerance (complex128 1e-12, complex64 1e-5)."""
+tolerance (complex128 1e-12, complex64 1e-5).  In NQPU_MODE_AUTO every gate run
+between measurements makes its own mode choice (22 qubits: tensor passes)."""
 import ctypes as C
 
 import numpy as np
@@ -30,7 +31,8 @@ def mid_circuit(n, seed):
 
 
 @pytest.mark.parametrize("n,dtype,mode", [(6, "c128", "tiled"), (6, "c128", "pergate"), (11, "c128", "tiled"),
-                                          (14, "c64", "tiled"), (14, "c64", "fused")])
+                                          (14, "c64", "tiled"), (14, "c64", "fused"), (14, "c64", "tensor"),
+                                          (22, "c64", "auto")])
 def test_measured_circuit_matches_oracle(n, dtype, mode):
     lib = _lib.load()
     for seed in (3, 4, 5):
