@@ -329,14 +329,17 @@ def run_engine(args):
                               "frac": fl / pass_s / 1e12 / tensor_peak(), "flops_per_step": fl // args.steps,
                               "peak_kind": "measured dense bf16 (cuBLAS burst); FP16 runs at the same rate"}
     elif args.mode == "tiled":
-        # the tiled pass is bound by FP32 issue, not HBM: its arithmetic rate against
-        # the FP32 peak (148 SMs x 128 lanes x 2 flops per cycle at the sampled clock)
+        # the tiled pass is bound by arithmetic issue, not HBM: its rate against the
+        # FP32 peak (148 SMs x 128 lanes x 2 flops per cycle at the sampled clock) for
+        # complex64, the FP64 peak (148 SMs x 64 lanes x 2) for complex128
         from nqpu_b200.circuits import algorithmic_flops
-        fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        lanes = 128 if args.dtype == "c64" else 64
+        arith_peak = 148 * lanes * 2 * mhz * 1e6 / 1e12
         fl = algorithmic_flops(gates, n) * args.steps
-        roofline["fp32"] = {"achieved_tflops": fl / pass_s / 1e12, "peak_tflops": fp32_peak,
-                            "frac": fl / pass_s / 1e12 / fp32_peak, "flops_per_step": fl // args.steps,
-                            "peak_kind": "nominal at the sampled SM clock"}
+        roofline["fp32" if args.dtype == "c64" else "fp64"] = {
+            "achieved_tflops": fl / pass_s / 1e12, "peak_tflops": arith_peak,
+            "frac": fl / pass_s / 1e12 / arith_peak, "flops_per_step": fl // args.steps,
+            "peak_kind": "nominal at the sampled SM clock"}
     launches_per_step = stats["passes"] + 1 + 2  # passes + reset + zsums (2 kernels)
 
     extra = {}
@@ -353,8 +356,19 @@ def run_engine(args):
             f = sv.fidelity(sv128)
             extra["accuracy_vs_fp64"] = {"one_minus_F": 1.0 - f, "max_abs_dZ": float(np.abs(z_c64 - z128).max()),
                                          "tolerance": {"one_minus_F": 1e-5, "max_abs_dZ": 1e-5}}
-            extra["complex128_run"] = {"gates_per_s": G / t128, "seconds": t128, "mode": mode128,
-                                       "passes": circ.plan_stats(n, "c128", mode128)["passes"]}
+            from nqpu_b200.circuits import algorithmic_flops
+            fl64 = algorithmic_flops(gates, n)
+            mhz64 = (clk or {}).get("sm_mhz") or 1965.0
+            # FP64 peak of the SIMT pipes: 148 SMs x 64 FP64 FMA lanes x 2 flops per cycle
+            fp64_peak = 148 * 64 * 2 * mhz64 * 1e6 / 1e12
+            passes128 = circ.plan_stats(n, "c128", mode128)["passes"]
+            extra["complex128_run"] = {
+                "gates_per_s": G / t128, "seconds": t128, "mode": mode128, "passes": passes128,
+                "hbm_GBps": passes128 * 2 * (1 << n) * 16 / t128 / 1e9,
+                "hbm_frac": passes128 * 2 * (1 << n) * 16 / t128 / 1e9 / peak,
+                "fp64": {"achieved_tflops": fl64 / t128 / 1e12, "peak_tflops": fp64_peak,
+                         "frac": fl64 / t128 / 1e12 / fp64_peak, "flops": fl64,
+                         "peak_kind": "nominal FP64 SIMT rate at the sampled SM clock"}}
             # the same circuit through the per-gate path in complex128 (one
             # kernel per gate, no planner): a check of the planned engine at
             # the full size that does not rest on the planner
