@@ -306,6 +306,14 @@ NqpuError    nqpu_circuit_profile(const NqpuCircuit* circuit, NqpuState* state, 
  * are built for the configuration in force when a circuit is first run on a
  * state size (a plan built for larger tiles is rebuilt, never run on smaller). */
 NqpuError    nqpu_tile_config_set(NqpuDtype dtype, uint32_t ctas_per_sm);
+/* Diagnostics (no counterpart in the reference): how many times a tensor-pass
+ * engine polls for its MMAs before it gives up (0 = the default, 2^22; at most
+ * 2^31 - 1).  never_arrives != 0 points that wait at a barrier nothing
+ * arrives on, so it expires: the failure injection of the tests.  On expiry
+ * the run returns NQPU_SIMULATION_FAILED; the engine still waits up to 2^24
+ * polls for its MMAs in flight before its CTA exits, and the next run starts
+ * with a cleared error flag.  Process-wide. */
+NqpuError    nqpu_tensor_wait_limit_set(uint32_t polls, int32_t never_arrives);
 uint32_t     nqpu_tile_config_get(NqpuDtype dtype);
 /* Plan statistics of the last execution of `circuit` in `mode` on an n-qubit state:
  * out[0] = HBM passes (kernel launches over the full state), out[1] = lowered ops,

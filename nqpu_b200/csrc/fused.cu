@@ -584,6 +584,8 @@ cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events
   ae = attr.get(dev, [] { return cudaFuncSetAttribute(k_fused_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFused); },
                 cudaErrorInvalidDevice);
   if (ae != cudaSuccess) return ae;
+  // the expiry flag of an earlier run is cleared, so this run reports its own
+  if ((ae = cudaMemsetAsync(p->d_err, 0, sizeof(int), s->stream)) != cudaSuccess) return ae;
   const int n = p->n;
   const uint64_t n_tiles = 1ull << (n - 12);
   const unsigned grid = unsigned(std::min<uint64_t>(n_tiles, uint64_t(p->norm_slots)));

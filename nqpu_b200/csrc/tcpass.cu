@@ -37,6 +37,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -78,7 +79,7 @@ static_assert(kTcParts % kTcBatch == 0, "whole batches");
 constexpr uint32_t kTcAPlane = 128 * 128;            // 16 KB: 128 rows x 64 halves
 constexpr uint32_t kTcOpBytes = 2 * kTcAPlane;       // hi + lo planes
 constexpr uint32_t kTcBBytes = 128 * 128;            // [B_hi; B_lo]: 128 rows x 64 halves
-constexpr uint32_t kTcWaitLimit = 1u << 22;          // bounded mbarrier polls
+constexpr uint32_t kTcWaitLimit = 1u << 22;          // bounded mbarrier polls (default)
 constexpr uint32_t kTcTmemCols = 512;                // the engines' accumulators (allocated as a power of two)
 
 // Every offset the kernel forms is GF(2)-linear in the bits of its index (the
@@ -130,7 +131,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_pass(float* __restrict__ amp, const TcPassRec* __restrict__ pass, const uint16_t* __restrict__ bmats,
               uint32_t n_tiles, float state_scale, const double* __restrict__ norm0,
               double* __restrict__ norm0_out, const double* __restrict__ prev_norm, int n_prev,
-              double* __restrict__ out_norm, int* __restrict__ err) {
+              double* __restrict__ out_norm, int* __restrict__ err, uint32_t wait_limit) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw_s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_raw));
   unsigned char* base_p = smem_raw + ((1024 - (raw_s & 1023)) & 1023);
@@ -139,6 +140,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   TcTables* T = reinterpret_cast<TcTables*>(bbuf + kTcMaxUnitaries * kTcBBytes);
   __shared__ TcPassRec P;
   __shared__ __align__(8) uint64_t mbar[kTcEngines];
+  __shared__ __align__(8) uint64_t mbar_never;  // failure injection: a barrier nothing arrives on
   __shared__ uint32_t tmem_holder;
   __shared__ int s_abort[kTcEngines];
   __shared__ float s_scale_in;
@@ -180,6 +182,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     mbar_init(mbar_s + 8u * uint32_t(tid), 1);
     s_abort[tid] = 0;
   }
+  const uint32_t never_s = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar_never));
+  if (tid == 0) mbar_init(never_s, 1);
+  // wait_limit: polls of the first MMA wait; bit 31 points that wait at
+  // mbar_never, so it expires (tests of the error path)
+  const bool inject = (wait_limit >> 31) != 0;
+  const uint32_t first_limit = wait_limit & 0x7FFFFFFFu;
   if (warp == 0) {
     const uint32_t holder = static_cast<uint32_t>(__cvta_generic_to_shared(&tmem_holder));
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(holder),
@@ -363,12 +371,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // named barrier below without taking issue slots
         uint32_t it = 0;
         bool done = false;
-        while (!(done = mbar_try_wait(my_mbar, phase)) && ++it < kTcWaitLimit) {
+        const uint32_t wait_bar = inject ? never_s : my_mbar;
+        while (!(done = mbar_try_wait(wait_bar, inject ? 0u : phase)) && ++it < first_limit) {
         }
         if (!done) {
           atomicExch(err, 1);
           s_abort[e] = 1;
-          // the MMAs may still be running: one more bounded wait before this
+          // the MMAs may still be running: one more bounded wait (of the
+          // default length, whatever the first wait's limit) before this
           // engine stops and the CTA's normal exit frees the accumulators
           for (uint32_t w = 0; w < 4 * kTcWaitLimit && !mbar_try_wait(my_mbar, phase); ++w) {
           }
@@ -565,6 +575,13 @@ void tc_plan_free(void* plan) {
   delete p;
 }
 
+// Polls of an engine's first wait for its MMAs before it gives up (sets the
+// error flag, then waits up to 4 x the default for the MMAs in flight, so
+// that no MMA outlives the CTA's tensor memory).  Bit 31 makes that first
+// wait poll a barrier nothing arrives on, so it expires: the failure
+// injection of nqpu_tensor_wait_limit_set.
+std::atomic<uint32_t> g_tc_wait_limit{kTcWaitLimit};
+
 cudaError_t tc_launch(float* amp, const TcPlan& plan, const TcPassRec* d_passes, const uint16_t* d_bmats,
                       const size_t* bmat_off, double* d_norm, int slots, int* d_err, cudaStream_t st,
                       std::vector<cudaEvent_t>* events) {
@@ -575,6 +592,9 @@ cudaError_t tc_launch(float* amp, const TcPlan& plan, const TcPassRec* d_passes,
   e = attr.get(dev, [] { return cudaFuncSetAttribute(k_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)); },
                cudaErrorInvalidDevice);
   if (e != cudaSuccess) return e;
+  // the expiry flag of an earlier run is cleared, so this run reports its own
+  if ((e = cudaMemsetAsync(d_err, 0, sizeof(int), st)) != cudaSuccess) return e;
+  const uint32_t wait_limit = g_tc_wait_limit.load(std::memory_order_relaxed);
   const uint32_t n_tiles = uint32_t(1) << (plan.n - kTcTileBits);
   const unsigned grid =
       unsigned(std::min<uint64_t>((uint64_t(n_tiles) + kTcEngines - 1) / kTcEngines, uint64_t(slots)));
@@ -584,7 +604,7 @@ cudaError_t tc_launch(float* amp, const TcPlan& plan, const TcPassRec* d_passes,
     const double* prevn = i ? d_norm + (1 + ((i + 1) & 1)) * size_t(slots) : nullptr;
     k_tc_pass<<<grid, kTcThreads, kTcSmem, st>>>(amp, d_passes + i, d_bmats + bmat_off[i], n_tiles, plan.state_scale,
                                                   i ? norm0 : nullptr, i ? nullptr : norm0, prevn, int(grid), outn,
-                                                  d_err);
+                                                  d_err, wait_limit);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (events) {
       cudaEvent_t ev;
@@ -623,3 +643,11 @@ cudaError_t tc_check_error(void* plan, cudaStream_t st) {
 }
 
 }  // namespace nqpu
+
+// Diagnostics: the tensor passes' first MMA wait (0 polls = the default).
+extern "C" NqpuError nqpu_tensor_wait_limit_set(uint32_t polls, int32_t never_arrives) {
+  if (polls > 0x7FFFFFFFu) return NQPU_INVALID_PARAMETER;
+  const uint32_t v = (polls ? polls : nqpu::kTcWaitLimit) | (never_arrives ? 0x80000000u : 0u);
+  nqpu::g_tc_wait_limit.store(v, std::memory_order_relaxed);
+  return NQPU_OK;
+}

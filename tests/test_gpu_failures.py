@@ -14,15 +14,21 @@ made on the host, never by faulting the GPU:
 * server: nqpu_server_wait with a timeout shorter than the request returns
   NQPU_SIMULATION_FAILED and the request still completes; nqpu_server_cancel
   withdraws a queued request.
+* tensor passes: nqpu_tensor_wait_limit_set(64, 1) points every engine's first
+  wait for its MMAs at a barrier nothing arrives on; the waits expire after 64
+  polls, each engine waits out its MMAs in flight and stops, and the run
+  returns NQPU_SIMULATION_FAILED.  With the default restored, the same circuit
+  and plan run again and match the oracle.
 """
 import numpy as np
 import pytest
 
-from nqpu_b200 import circuits
+from nqpu_b200 import _lib, circuits
 from nqpu_b200._lib import NqpuErrorException
 from nqpu_b200.batch import Batch
 from nqpu_b200.server import Server
-from nqpu_b200.state import Circuit
+from nqpu_b200.state import Circuit, StateVector
+from oracle.oracle import OracleState
 
 pytestmark = pytest.mark.gpu
 
@@ -112,3 +118,26 @@ def test_server_cancel_queued_request():
         st = srv.stats()
         assert st["cancelled"] == 1 and st["completed"] == 2 and st["failed"] == 0
         assert srv.lib.nqpu_server_cancel(srv.h_, 12345) == INVALID_HANDLE  # unknown id
+
+
+def test_tensor_pass_wait_expiry_is_reported_and_the_plan_recovers():
+    lib = _lib.load()
+    n = 14
+    gates = circuits.brickwork(n, 6, 3)
+    c = Circuit(n, gates)
+    tensor = 3  # NQPU_MODE_TENSOR
+    try:
+        assert lib.nqpu_tensor_wait_limit_set(64, 1) == 0
+        with StateVector(n, "c64") as sv:
+            assert lib.nqpu_circuit_execute_ex(c.h_, sv.h_, tensor) == SIMULATION_FAILED
+    finally:
+        assert lib.nqpu_tensor_wait_limit_set(0, 0) == 0
+    o = OracleState(n)
+    o.apply(gates)
+    ref = o.amplitudes()
+    with StateVector(n, "c64") as sv:
+        assert lib.nqpu_circuit_execute_ex(c.h_, sv.h_, tensor) == 0  # the cached plan, error flag cleared
+        got = sv.amplitudes()
+    fid = abs(np.vdot(ref, got)) ** 2
+    assert 1 - fid <= 1e-5
+    assert lib.nqpu_tensor_wait_limit_set(1 << 31, 0) == 2  # beyond the limit's range
