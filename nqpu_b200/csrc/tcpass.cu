@@ -40,6 +40,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "device_once.h"
@@ -410,67 +411,75 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // column c = kTcCols ch + 4 part + cc (+ 1 for the second amplitude of
       // a pair): its offsets are the XOR (operand) / sum (amplitude) of one
       // table entry per set bit
-      uint32_t xb[5];
-      uint64_t gb[5];
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        xb[i] = T->xcb[j][i];
-        gb[i] = last ? T->gcb[j][i] : 0ull;
-      }
-      uint32_t xbase = my_ptn;
-      uint64_t gbase = tb + pg;
-      if (kTcColHalves == 2 && ch) {
-        xbase ^= xb[4];
-        gbase += gb[4];
-      }
-      float2* out = reinterpret_cast<float2*>(amp) + gbase;
       float2 nout = make_float2(0.0f, 0.0f);
-      const float scv = last ? out_scale : mid_scale;
-      const float2 sc = make_float2(scv, scv);
+      // the mid epilogues need only the operand offsets, the last one only
+      // the amplitude offsets: two compile-time forms of the drain loop
+      auto drain = [&](auto last_c) {
+        constexpr bool kLast = decltype(last_c)::value;
+        uint32_t xb[5];
+        uint64_t gb[5];
 #pragma unroll
-      for (int pb = 0; pb < kTcParts; pb += kTcBatch) {
-        uint32_t rh[kTcBatch][8];
+        for (int i = 0; i < 5; ++i) {
+          if constexpr (kLast) gb[i] = T->gcb[j][i];
+          else xb[i] = T->xcb[j][i];
+        }
+        uint32_t xbase = my_ptn;
+        uint64_t gbase = tb + pg;
+        if (kTcColHalves == 2 && ch) {
+          if constexpr (kLast) gbase += gb[4];
+          else xbase ^= xb[4];
+        }
+        float2* out = reinterpret_cast<float2*>(amp) + gbase;
+        const float scv = kLast ? out_scale : mid_scale;
+        const float2 sc = make_float2(scv, scv);
 #pragma unroll
-        for (int k = 0; k < kTcBatch; ++k) tmem_ld8(lanes + 8u * uint32_t(pb + k), rh[k]);
-        tmem_ld_wait();
+        for (int pb = 0; pb < kTcParts; pb += kTcBatch) {
+          uint32_t rh[kTcBatch][8];
 #pragma unroll
-        for (int k = 0; k < kTcBatch; ++k) {
+          for (int k = 0; k < kTcBatch; ++k) tmem_ld8(lanes + 8u * uint32_t(pb + k), rh[k]);
+          tmem_ld_wait();
 #pragma unroll
-          for (int cc = 0; cc < 4; cc += 2) {
-            const int cb = 4 * (pb + k) + cc;  // column bits below the column half (compile time)
-            uint32_t xo = 0;
-            uint64_t go = 0;
+          for (int k = 0; k < kTcBatch; ++k) {
 #pragma unroll
-            for (int b = 1; b < 5; ++b)
-              if ((cb >> b) & 1) {
-                xo ^= xb[b];
-                go += gb[b];
-              }
-            // out = D * scale, packed (re, im)
-            const float2 x0 = __fmul2_rn(make_float2(__uint_as_float(rh[k][2 * cc]), __uint_as_float(rh[k][2 * cc + 1])), sc);
-            const float2 x1 =
-                __fmul2_rn(make_float2(__uint_as_float(rh[k][2 * cc + 2]), __uint_as_float(rh[k][2 * cc + 3])), sc);
-            if (!last) {
-              const uint32_t o0 = xbase ^ xo;
-              if (my_pair) {
-                put2(o0, x0, x1);
+            for (int cc = 0; cc < 4; cc += 2) {
+              const int cb = 4 * (pb + k) + cc;  // column bits below the column half (compile time)
+              // out = D * scale, packed (re, im)
+              const float2 x0 =
+                  __fmul2_rn(make_float2(__uint_as_float(rh[k][2 * cc]), __uint_as_float(rh[k][2 * cc + 1])), sc);
+              const float2 x1 =
+                  __fmul2_rn(make_float2(__uint_as_float(rh[k][2 * cc + 2]), __uint_as_float(rh[k][2 * cc + 3])), sc);
+              if constexpr (!kLast) {
+                uint32_t xo = 0;
+#pragma unroll
+                for (int b = 1; b < 5; ++b)
+                  if ((cb >> b) & 1) xo ^= xb[b];
+                const uint32_t o0 = xbase ^ xo;
+                if (my_pair) {
+                  put2(o0, x0, x1);
+                } else {
+                  put1(o0, x0);
+                  put1(o0 ^ xb[0], x1);
+                }
               } else {
-                put1(o0, x0);
-                put1(o0 ^ xb[0], x1);
-              }
-            } else {
-              nout = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nout));
-              float2* o0 = out + go;
-              if (store16) {
-                __stcs(reinterpret_cast<float4*>(o0), make_float4(x0.x, x0.y, x1.x, x1.y));
-              } else {
-                __stcs(o0, x0);
-                __stcs(o0 + gb[0], x1);
+                uint64_t go = 0;
+#pragma unroll
+                for (int b = 1; b < 5; ++b)
+                  if ((cb >> b) & 1) go += gb[b];
+                nout = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nout));
+                float2* o0 = out + go;
+                if (store16) {
+                  __stcs(reinterpret_cast<float4*>(o0), make_float4(x0.x, x0.y, x1.x, x1.y));
+                } else {
+                  __stcs(o0, x0);
+                  __stcs(o0 + gb[0], x1);
+                }
               }
             }
           }
         }
-      }
+      };
+      if (last) drain(std::true_type{});
+      else drain(std::false_type{});
       if (last) norm_out += double(nout.x) + double(nout.y);
       else fence_proxy_async_smem();
       engine_barrier();  // the accumulator is drained before the next MMAs overwrite it
