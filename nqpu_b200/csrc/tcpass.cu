@@ -5,7 +5,7 @@
 // Per pass, one persistent CTA per SM with four independent tile engines of
 // four warps (one per TMEM lane quadrant).  An engine owns an operand buffer
 // (the tile as the 128 x 64 FP16 A operand: hi and lo planes, K-major,
-// 128-byte swizzle, 32 KB) and a 128-column TMEM accumulator, and runs its
+// 128-byte swizzle, 32 KB) and a 64-column TMEM accumulator, and runs its
 // tiles through:
 //   load     the tile's 32 KB (128 runs of 32 contiguous amplitudes) arrive
 //            by 16-byte cp.async as raw FP32 in the engine's own operand
@@ -27,7 +27,9 @@
 //            the last unitary, stores out / s to HBM.
 // While one engine waits for its MMAs the other three run, so the tensor
 // pipe, shared memory and HBM overlap across four tiles.  The B operands of
-// the pass's unitaries stay in shared memory for the launch.
+// the pass's unitaries stay in shared memory for the launch.  The stores
+// follow the pass's store-side index bits (qt_out), which may place the tile's
+// qubits on other state index bits than it loaded them from (see tcpass.h).
 //
 // Renormalisation: the first pass of a run records the FP64 norm of its input
 // (per-CTA partials) and every pass the norm of its output; each later pass
@@ -363,7 +365,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     engine_barrier();
     bool aborted = false;
     for (int j = 0; j < m; ++j) {
-      // ---- unitary j on the tensor cores: 8 MMAs of K = 16 ----
+      // ---- unitary j on the tensor cores: 12 MMAs of K = 16, N = 64 ----
       if (et == 0) {
         // the descriptors differ only in their start-address field (address
         // >> 4), which these offsets do not carry out of
