@@ -76,8 +76,38 @@ void state_free(StateImpl* s) {
   if (s->h_small) cudaFreeHost(s->h_small);
   if (s->d_uni) cudaFree(s->d_uni);
   if (s->d_shots) cudaFree(s->d_shots);
+  if (s->run_norm) cudaFree(s->run_norm);
+  if (s->run_err) cudaFree(s->run_err);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
+}
+
+cudaError_t state_run_scratch(StateImpl* s, size_t doubles, double** norm, int** err) {
+  cudaError_t e;
+  if (s->run_norm_cap < doubles) {
+    // the old buffer may back a run still queued on the state's stream
+    if (s->run_norm && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return e;
+    if (s->run_norm) cudaFree(s->run_norm);
+    s->run_norm = nullptr;
+    s->run_norm_cap = 0;
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&s->run_norm), doubles * sizeof(double))) != cudaSuccess) return e;
+    s->run_norm_cap = doubles;
+  }
+  if (!s->run_err && (e = cudaMalloc(reinterpret_cast<void**>(&s->run_err), sizeof(int))) != cudaSuccess) return e;
+  // the expiry flag of an earlier run is cleared, so this run reports its own
+  if ((e = cudaMemsetAsync(s->run_err, 0, sizeof(int), s->stream)) != cudaSuccess) return e;
+  *norm = s->run_norm;
+  *err = s->run_err;
+  return cudaSuccess;
+}
+
+cudaError_t state_run_error(StateImpl* s) {
+  if (!s->run_err) return cudaSuccess;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, s->run_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return e;
+  return h ? cudaErrorLaunchTimeout : cudaSuccess;
 }
 
 cudaError_t state_zsums(const StateImpl* s, double* zs, double* total) {
@@ -482,12 +512,12 @@ static cudaError_t segment_run(CircuitImpl* c, const Segment& seg, int si, State
   if (effective == NQPU_MODE_FUSED) {
     e = fused_run(p->fused, s, events);
     if (e != cudaSuccess) return e;
-    return fused_check_error(p->fused, s->stream);  // bounded-wait expiry flag
+    return state_run_error(s);  // bounded-wait expiry flag
   }
   if (effective == NQPU_MODE_TENSOR) {
     e = tc_run(p->tc, s, events);
     if (e != cudaSuccess) return e;
-    return tc_check_error(p->tc, s->stream);  // bounded-wait expiry flag
+    return state_run_error(s);  // bounded-wait expiry flag
   }
   for (size_t i = 0; i < p->tile.passes.size(); ++i) {
     e = launch_tile_pass(s->dt, s->amp, int(s->n), p->tile.passes[i], p->d_passes, p->d_stages,

@@ -32,10 +32,22 @@ struct StateImpl {
   double* d_uni = nullptr;     // sampling uniforms
   uint64_t* d_shots = nullptr; // sampling outcomes
   uint32_t shot_cap = 0;
+  // scratch of the tensor and fused passes (per state, so one circuit run on
+  // two states whose streams overlap does not share it): per-CTA norm
+  // partials and the bounded-wait expiry flag
+  double* run_norm = nullptr;
+  size_t run_norm_cap = 0;     // doubles
+  int* run_err = nullptr;
 };
 
 StateImpl* state_new(uint32_t n, DType dt);
 void state_free(StateImpl* s);
+// The state's run scratch with room for `doubles` norm partials (grown on
+// demand), its expiry flag cleared on the state's stream.
+cudaError_t state_run_scratch(StateImpl* s, size_t doubles, double** norm, int** err);
+// cudaErrorLaunchTimeout when the last tensor / fused run's bounded wait
+// expired (synchronises the state's stream).
+cudaError_t state_run_error(StateImpl* s);
 // out (n+1 values): [0] = sum|a|^2, [1+q] = sum over bit q set; either pointer may be null.
 cudaError_t state_zsums(const StateImpl* s, double* zs, double* total);
 cudaError_t state_pauli(const StateImpl* s, uint64_t xm, uint64_t zm, uint64_t ym, double* out2);

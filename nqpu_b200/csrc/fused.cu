@@ -421,9 +421,7 @@ struct FusedPlanImpl {
   std::vector<FusedGate> gates;
   std::vector<FusedArgs> args;
   float* d_bmats = nullptr;  // per gate: hi[64][64], lo[64][64]
-  double* d_norm = nullptr;  // two buffers of per-CTA norm partials (ping-pong)
-  int norm_slots = 0;
-  int* d_err = nullptr;
+  int norm_slots = 0;  // per-CTA norm partials per launch (the state holds two buffers, ping-pong)
 };
 
 static void real_embedding(const FusedGate& g, float* hi, float* lo) {
@@ -549,9 +547,6 @@ bool fused_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, 
   bool ok = cudaMalloc(reinterpret_cast<void**>(&p->d_bmats), host.size() * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMemcpy(p->d_bmats, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess;
   p->norm_slots = device_sms() * kFusedCtasPerSm;
-  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_norm), sizeof(double) * 2 * p->norm_slots) == cudaSuccess;
-  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_err), sizeof(int)) == cudaSuccess;
-  ok = ok && cudaMemset(p->d_err, 0, sizeof(int)) == cudaSuccess;
   if (!ok) {
     fused_plan_free(p);
     return false;
@@ -568,8 +563,6 @@ void fused_plan_free(void* plan) {
   auto* p = static_cast<FusedPlanImpl*>(plan);
   if (!p) return;
   if (p->d_bmats) cudaFree(p->d_bmats);
-  if (p->d_norm) cudaFree(p->d_norm);
-  if (p->d_err) cudaFree(p->d_err);
   delete p;
 }
 
@@ -584,19 +577,21 @@ cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events
   ae = attr.get(dev, [] { return cudaFuncSetAttribute(k_fused_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFused); },
                 cudaErrorInvalidDevice);
   if (ae != cudaSuccess) return ae;
-  // the expiry flag of an earlier run is cleared, so this run reports its own
-  if ((ae = cudaMemsetAsync(p->d_err, 0, sizeof(int), s->stream)) != cudaSuccess) return ae;
+  // norm partials and expiry flag of this run: the state's scratch
+  double* d_norm = nullptr;
+  int* d_err = nullptr;
+  if ((ae = state_run_scratch(s, 2 * size_t(p->norm_slots), &d_norm, &d_err)) != cudaSuccess) return ae;
   const int n = p->n;
   const uint64_t n_tiles = 1ull << (n - 12);
   const unsigned grid = unsigned(std::min<uint64_t>(n_tiles, uint64_t(p->norm_slots)));
   cudaError_t e = cudaSuccess;
   int prev_grid = 0;
   for (size_t i = 0; i < p->gates.size(); ++i) {
-    double* outn = p->d_norm + (i & 1) * p->norm_slots;
-    const double* prevn = i ? p->d_norm + ((i + 1) & 1) * p->norm_slots : nullptr;
+    double* outn = d_norm + (i & 1) * p->norm_slots;
+    const double* prevn = i ? d_norm + ((i + 1) & 1) * p->norm_slots : nullptr;
     k_fused_apply<<<grid, kFusedThreads, kSmemFused, s->stream>>>(
         static_cast<float*>(s->amp), p->args[i], p->d_bmats + i * 8192, prevn, prev_grid, outn, n_tiles,
-        p->d_err);
+        d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     prev_grid = int(grid);
     if (events) {
@@ -609,14 +604,5 @@ cudaError_t fused_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events
   return cudaSuccess;
 }
 
-cudaError_t fused_check_error(void* plan, cudaStream_t st) {
-  auto* p = static_cast<FusedPlanImpl*>(plan);
-  if (!p) return cudaSuccess;
-  int h = 0;
-  cudaError_t e = cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return e;
-  return h ? cudaErrorLaunchTimeout : cudaSuccess;
-}
 
 }  // namespace nqpu

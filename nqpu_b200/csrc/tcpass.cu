@@ -549,9 +549,6 @@ struct TcPlanImpl {
   std::vector<size_t> bmat_off;   // first B-operand half of each pass
   TcPassRec* d_passes = nullptr;
   uint16_t* d_bmats = nullptr;
-  double* d_norm = nullptr;       // [norm0 | out ping | out pong], `slots` doubles each
-  int slots = 0;
-  int* d_err = nullptr;
 };
 
 bool tc_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, PlanStats* stats) {
@@ -577,10 +574,6 @@ bool tc_plan_build(const std::vector<Op>& ops, int n, DType dt, void** plan, Pla
                     cudaMemcpyHostToDevice) == cudaSuccess;
   if (ok && off)
     ok = cudaMemcpy(p->d_bmats, p->plan.bmats.data(), off * sizeof(uint16_t), cudaMemcpyHostToDevice) == cudaSuccess;
-  p->slots = device_sms();
-  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_norm), sizeof(double) * 3 * size_t(p->slots)) == cudaSuccess;
-  ok = ok && cudaMalloc(reinterpret_cast<void**>(&p->d_err), sizeof(int)) == cudaSuccess;
-  ok = ok && cudaMemset(p->d_err, 0, sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     tc_plan_free(p);
@@ -605,8 +598,6 @@ void tc_plan_free(void* plan) {
   if (!p) return;
   if (p->d_passes) cudaFree(p->d_passes);
   if (p->d_bmats) cudaFree(p->d_bmats);
-  if (p->d_norm) cudaFree(p->d_norm);
-  if (p->d_err) cudaFree(p->d_err);
   delete p;
 }
 
@@ -663,19 +654,17 @@ void tc_bmat_offsets(const TcPlan& plan, std::vector<size_t>* off) {
 cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events) {
   auto* p = static_cast<TcPlanImpl*>(plan);
   if (!p || s->dt != DType::C64 || int(s->n) != p->plan.n) return cudaErrorInvalidValue;
-  return tc_launch(static_cast<float*>(s->amp), p->plan, p->d_passes, p->d_bmats, p->bmat_off.data(), p->d_norm,
-                   p->slots, p->d_err, s->stream, events);
+  // norm partials ([norm0 | out ping | out pong], one slot per CTA) and the
+  // expiry flag of this run: the state's scratch
+  const int slots = device_sms();
+  double* norm = nullptr;
+  int* err = nullptr;
+  const cudaError_t e = state_run_scratch(s, 3 * size_t(slots), &norm, &err);
+  if (e != cudaSuccess) return e;
+  return tc_launch(static_cast<float*>(s->amp), p->plan, p->d_passes, p->d_bmats, p->bmat_off.data(), norm, slots,
+                   err, s->stream, events);
 }
 
-cudaError_t tc_check_error(void* plan, cudaStream_t st) {
-  auto* p = static_cast<TcPlanImpl*>(plan);
-  if (!p) return cudaSuccess;
-  int h = 0;
-  cudaError_t e = cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return e;
-  return h ? cudaErrorLaunchTimeout : cudaSuccess;
-}
 
 }  // namespace nqpu
 

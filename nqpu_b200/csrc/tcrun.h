@@ -13,8 +13,6 @@ bool tc_plan_stats(const std::vector<Op>& ops, int n, DType dt, PlanStats* stats
 void tc_plan_free(void* plan);
 // Queue every pass of the plan on the state's stream (one launch per pass).
 cudaError_t tc_run(void* plan, StateImpl* s, std::vector<cudaEvent_t>* events);
-// Reads the plan's device error flag (set when a bounded wait expired).
-cudaError_t tc_check_error(void* plan, cudaStream_t st);
 // Queue the passes of a host plan whose records and B operands are already in
 // device memory: pass i's record at d_passes + i, its B operands at d_bmats +
 // bmat_off[i] (tc_bmat_offsets); d_norm holds 3 * slots doubles of scratch

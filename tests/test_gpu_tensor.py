@@ -161,3 +161,34 @@ def test_auto_mode_matches_oracle(n, kind, dtype):
     tol = TOL if dtype == "c64" else 1e-12
     assert 1 - fid(ref, got) <= tol
     assert np.abs(z - zref).max() <= max(tol, 1e-12)
+
+
+def test_one_circuit_on_two_states_at_once():
+    """The same circuit handle runs on two states from two host threads, so
+    the two runs overlap on the GPU; each run's norm partials and error flag
+    live in its own state, so both results equal a run on its own, bitwise."""
+    import threading
+    n = 22
+    c = Circuit(n, circuits.brickwork(n, 16, 9))
+    with StateVector(n, "c64") as sv:
+        c.execute(sv, "tensor")
+        alone = sv.amplitudes()
+    for _ in range(3):
+        svs = [StateVector(n, "c64"), StateVector(n, "c64")]
+        errs = []
+
+        def run(sv):
+            try:
+                c.execute(sv, "tensor")
+            except Exception as e:  # reported below
+                errs.append(e)
+
+        th = [threading.Thread(target=run, args=(s,)) for s in svs]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert not errs, errs
+        for s in svs:
+            assert np.array_equal(s.amplitudes(), alone)
+            s.close()
