@@ -130,6 +130,30 @@ __device__ __forceinline__ void split_pair(float2 x, uint32_t& hi, uint32_t& lo)
   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
+// Last epilogue: exchange lane bit l (lmask = 1 << l) with column bit KC of a
+// 16-column batch across the warp.  Lane t's register of column c then holds
+// the element of lane t with bit l set to c's bit KC, column c with bit KC set
+// to t's bit l: the lane with bit l set sends its column of bit KC = 0 and
+// takes its partner's column of bit KC = 1 in its place, the partner the
+// reverse (one shuffle per register pair).
+static_assert(kTcBatch == 4 && kTcColHalves == 1, "lane exchanges: column bits 1..3 inside a batch, one thread per row");
+template <int KC>
+__device__ __forceinline__ void lane_swap(uint32_t (&rh)[kTcBatch][8], uint32_t lmask, bool up) {
+#pragma unroll
+  for (int c = 0; c < 4 * kTcBatch; ++c) {
+    if (c & (1 << KC)) continue;
+    const int c2 = c | (1 << KC);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t& a = rh[c >> 2][2 * (c & 3) + h];
+      uint32_t& b = rh[c2 >> 2][2 * (c2 & 3) + h];
+      const uint32_t r = __shfl_xor_sync(0xffffffffu, up ? a : b, lmask);
+      if (up) a = r;
+      else b = r;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_pass(float* __restrict__ amp, const TcPassRec* __restrict__ pass, const uint16_t* __restrict__ bmats,
               uint32_t n_tiles, float state_scale, const double* __restrict__ norm0,
@@ -174,7 +198,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (tid < 5 * m) {
     const int j = tid / 5, i = tid % 5;
     T->xcb[j][i] = j + 1 < m ? P.u[j + 1].boff[P.u[j].fcol[i]] : 0u;
-    T->gcb[j][i] = 1ull << P.qt_out[P.u[j].fcol[i]];
+    // the last epilogue's column bit 1 + s stores to the index bit of lane bit
+    // sw_lane[s] after the lane exchange
+    int sb = P.qt_out[P.u[j].fcol[i]];
+    if (j + 1 == m && i >= 1 && i <= 3 && P.sw_lane[i - 1] >= 0) sb = P.qt_out[P.u[j].frow[P.sw_lane[i - 1]]];
+    T->gcb[j][i] = 1ull << sb;
   }
   if (tid < kTcStpBits) {
     T->sob[tid] = P.u[0].boff[P.lt[kTcThrBits + tid]];
@@ -254,7 +282,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       pair[j] = P.u[j + 1].boff[P.u[j].fcol[0]] == 4u;
     } else if (j + 1 == m) {
       for (int i = 0; i < 7; ++i)
-        if ((row >> i) & 1u) pg |= 1ull << P.qt_out[P.u[j].frow[i]];
+        if ((row >> i) & 1u) {
+          int sb = P.qt_out[P.u[j].frow[i]];
+          for (int s = 0; s < 3; ++s)
+            if (P.sw_lane[s] == i) sb = P.qt_out[P.u[j].fcol[1 + s]];  // exchanged with column bit 1 + s
+          pg |= 1ull << sb;
+        }
     }
   }
   const bool store16 = P.qt_out[P.u[m - 1].fcol[0]] == 0;  // index bit 0 is column bit 0 of the last layout
@@ -456,6 +489,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
           for (int k = 0; k < kTcBatch; ++k) tmem_ld8(lanes + 8u * uint32_t(pb + k), rh[k]);
           tmem_ld_wait();
+          if constexpr (kLast) {
+            // low index bits onto lanes: whole 128-byte lines per warp store
+            // (the exchanges are read from the shared pass record here, so no
+            // register holds them across the drain)
+            const int s0 = P.sw_lane[0], s1 = P.sw_lane[1], s2 = P.sw_lane[2];
+            if (s0 >= 0) lane_swap<1>(rh, 1u << s0, (lane >> s0) & 1);
+            if (s1 >= 0) lane_swap<2>(rh, 1u << s1, (lane >> s1) & 1);
+            if (s2 >= 0) lane_swap<3>(rh, 1u << s2, (lane >> s2) & 1);
+          }
 #pragma unroll
           for (int k = 0; k < kTcBatch; ++k) {
 #pragma unroll

@@ -64,8 +64,30 @@ struct TcPassRec {
   // are tile bits 1..3, so 8 lanes read 128 contiguous bytes) and of load-step
   // bit b - kTcLoadThreadBits; tile bit 0 is the pair inside each 16-byte load
   int32_t lt[11];
+  // last epilogue: lane (row) bit exchanged with column bit 1 + s of the last
+  // unitary by a shuffle before the HBM stores, or -1 (see tc_store_bits)
+  int32_t sw_lane[3];
   TcUnitaryRec u[kTcMaxUnitaries];
 };
+
+// State index bit that row bit i / column bit i of the last unitary stores to.
+// The last epilogue holds D one row per lane; before its HBM stores, swap s
+// exchanges lane bit sw_lane[s] with column bit 1 + s across the warp (lane
+// l's register for column c then holds the amplitude of row l with that bit
+// set to c's bit, column c with that bit set to l's), so that the low index
+// bits of the state lie on lanes and each warp store covers whole 128-byte
+// lines.  In the address tables this is the exchange of the two bits' entries.
+inline void tc_store_bits(const TcPassRec& P, int32_t* row_bits, int32_t* col_bits) {
+  const TcUnitaryRec& U = P.u[P.m - 1];
+  for (int i = 0; i < 7; ++i) row_bits[i] = P.qt_out[U.frow[i]];
+  for (int i = 0; i < 5; ++i) col_bits[i] = P.qt_out[U.fcol[i]];
+  for (int s = 0; s < 3; ++s)
+    if (P.sw_lane[s] >= 0) {
+      const int32_t t = row_bits[P.sw_lane[s]];
+      row_bits[P.sw_lane[s]] = col_bits[1 + s];
+      col_bits[1 + s] = t;
+    }
+}
 
 // Qubit placement: a pass may store its tile with its qubits on other state
 // index bits than it loaded them from (qt_out), so that the qubits the next

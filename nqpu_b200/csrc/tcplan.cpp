@@ -82,6 +82,32 @@ int store_wavefronts(const int* lb, const uint32_t* boff, int width) {
   return 1 << (5 - rank5(v, 5));
 }
 
+// Lane exchanges of the last epilogue (TcPassRec::sw_lane): column bit 1 + s
+// of the last unitary, when it stores to index bit 0..3, trades places with
+// the free lane bit (row bits 0..4) that stores to the highest index bit >= 4.
+// Each exchange halves the 128-byte lines a warp store touches (a line holds
+// the 16 amplitudes that differ in index bits 0..3).  qt: store-side index
+// bits of the tile bits.
+int lane_swaps(const int* frow, const int* fcol, const int* qt, int32_t* sw) {
+  bool used[5] = {false, false, false, false, false};
+  int cnt = 0;
+  int order[3] = {1, 2, 3};  // column bits by their index bit, lowest first
+  std::sort(order, order + 3, [&](int a, int b) { return qt[fcol[a]] < qt[fcol[b]]; });
+  for (int s = 0; s < 3; ++s) sw[s] = -1;
+  for (int k = 0; k < 3; ++k) {
+    const int cb = order[k];
+    if (qt[fcol[cb]] > 3) continue;
+    int best = -1;
+    for (int i = 0; i < 5; ++i)
+      if (!used[i] && qt[frow[i]] >= 4 && (best < 0 || qt[frow[i]] > qt[frow[best]])) best = i;
+    if (best < 0) break;
+    used[best] = true;
+    sw[cb - 1] = best;
+    ++cnt;
+  }
+  return cnt;
+}
+
 // Layout choice of a pass: column order and row order of every unitary's
 // operand, and the loader's map from thread / step bits to tile bits.
 struct LayoutCfg {
@@ -91,9 +117,12 @@ struct LayoutCfg {
 };
 
 // Per-tile cost of a layout choice: shared-memory store wavefronts of the
-// loader and of the epilogues that feed the next unitary, plus a quarter unit
-// per 32-byte sector the last epilogue's HBM stores touch beyond the minimum
-// (partly written sectors still merge in L2 before they reach DRAM).
+// loader and of the epilogues that feed the next unitary, plus, for the last
+// epilogue's HBM stores (after its lane exchanges), a quarter unit per 32-byte
+// sector and four units per 128-byte line a warp store touches beyond the
+// minimum, and 256 units per lane exchange (its shuffles).  (Measured on the
+// 30-qubit brickwork: stores at 4 lines per warp instead of 10-11 shorten a
+// tile's last epilogue by 1000-3000 cycles.)
 int layout_cost(const LayoutCfg& c, int m, const int* qt) {
   uint32_t boff[kTcMaxUnitaries][12];
   for (int j = 0; j < m; ++j) layout_offsets(c.frow[j], c.fcol[j], boff[j]);
@@ -111,17 +140,27 @@ int layout_cost(const LayoutCfg& c, int m, const int* qt) {
     const bool pair = c.fcol[j][0] == c.fcol[j + 1][0];
     cost += 4 * (pair ? 16 : 32) * 2 * store_wavefronts(c.frow[j], boff[j + 1], pair ? 8 : 4);
   }
-  // HBM: lanes over rows 0..4 of the last layout.  A 32-byte sector holds the
-  // 4 amplitudes that differ in qubits 0 and 1 (tile bits 0 and 1), so a warp
-  // touches 32 / 2^k sectors when k of those tile bits are lane bits; the
-  // minimum is 8 for 8-byte stores and 16 for 16-byte ones (qubit 0 is then a
-  // column bit and each lane writes a pair).
+  // HBM: lanes over rows 0..4 of the last layout, after the lane exchanges.
+  // A warp store touches 2^k sectors (32 bytes: index bits 0, 1 inside) when k
+  // lane bits store to index bits >= 2, and 2^k' lines when k' of them store
+  // to index bits >= 4; the minima are 16 sectors / 4 lines for 16-byte
+  // stores (index bit 0 is column bit 0 and each lane writes a pair) and 8 / 2
+  // for 8-byte ones.
   const int L = m - 1;
   const bool wide = qt[c.fcol[L][0]] == 0;  // qt: the store-side index bits (qt_out)
-  int k = 0;
-  for (int i = 0; i < 5; ++i) k += qt[c.frow[L][i]] <= 1 ? 1 : 0;  // the row bit stores to index bit 0 or 1
-  const int ns = 32 >> k, ideal = wide ? 16 : 8;
-  cost += (4 * (wide ? 16 : 32) * (ns - ideal)) / 4;
+  int32_t sw[3];
+  const int nsw = lane_swaps(c.frow[L], c.fcol[L], qt, sw);
+  int lane_bit[5];
+  for (int i = 0; i < 5; ++i) lane_bit[i] = qt[c.frow[L][i]];
+  for (int s = 0; s < 3; ++s)
+    if (sw[s] >= 0) lane_bit[sw[s]] = qt[c.fcol[L][1 + s]];
+  int ks = 0, kl = 0;
+  for (int i = 0; i < 5; ++i) {
+    ks += lane_bit[i] >= 2 ? 1 : 0;
+    kl += lane_bit[i] >= 4 ? 1 : 0;
+  }
+  const int instr = 4 * (wide ? 16 : 32);
+  cost += instr * (((1 << ks) - (wide ? 16 : 8)) / 4 + 4 * ((1 << kl) - (wide ? 4 : 2))) + 256 * nsw;
   return cost;
 }
 
@@ -139,6 +178,13 @@ void choose_layouts(TcPassRec& P) {
     uint64_t fm = 0;
     for (int i = 0; i < 5; ++i) fm |= 1ull << P.u[j].fcol[i];
     key |= fm << (4 + 12 * j);
+  }
+  // the store cost depends on which tile bits store to index bits 0..3
+  for (int s = 0; s < 4; ++s) {
+    uint64_t tb = 15;
+    for (int b = 0; b < kTcTileBits; ++b)
+      if (P.qt_out[b] == s) tb = uint64_t(b);
+    key |= tb << (40 + 4 * s);
   }
   auto apply = [&](const LayoutCfg& best) {
     for (int j = 0; j < m; ++j) {
@@ -440,6 +486,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     TcPassRec P;
     std::memset(&P, 0, sizeof(P));
     P.m = int(clusters.size());
+    for (int s = 0; s < 3; ++s) P.sw_lane[s] = -1;
     std::array<int32_t, kTcTileBits> lq{};
     {
       // tile bits in the order of their index bits when loaded (bits 0..4
@@ -490,6 +537,9 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     TcPassRec& P = out->passes[pi];
     choose_layouts(P);
     for (int j = 0; j < P.m; ++j) layout_offsets(P.u[j].frow, P.u[j].fcol, P.u[j].boff);
+    lane_swaps(P.u[P.m - 1].frow, P.u[P.m - 1].fcol, P.qt_out, P.sw_lane);
+    int32_t st_row[7], st_col[5];
+    tc_store_bits(P, st_row, st_col);
     for (int j = 0; j < P.m; ++j) {
       TcUnitaryRec& U = P.u[j];
       for (uint32_t c = 0; c < 32; ++c) {
@@ -498,7 +548,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
         for (int i = 0; i < 5; ++i)
           if ((c >> i) & 1u) {
             if (j + 1 < P.m) x ^= P.u[j + 1].boff[U.fcol[i]];
-            g |= 1ull << P.qt_out[U.fcol[i]];
+            g |= 1ull << (j + 1 == P.m ? st_col[i] : P.qt_out[U.fcol[i]]);
           }
         U.xnext[c] = x;
         U.gcol[c] = g;

@@ -63,7 +63,8 @@ extern "C" uint16_t emu_half_bits(float x) { return tc_half_bits(x); }
 // Returns the number of passes (>= 0) or a negative error code:
 // -1 plan failed, -2 operand slot written twice / misaligned, -3 amplitude
 // written twice or not at all, -4 a pairing condition does not hold,
-// -5 the loader's bit map is not a permutation with tile bits 1..3 first.
+// -5 the loader's bit map is not a permutation with tile bits 1..3 first,
+// -6 the last epilogue's lane exchanges are not distinct lane bits 0..4.
 extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, int split, int64_t* stats) {
   std::vector<GateRec> gates(static_cast<size_t>(ngates));
   for (int i = 0; i < ngates; ++i) {
@@ -126,6 +127,19 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
       }
       if (P.lt[0] != 1 || P.lt[1] != 2 || P.lt[2] != 3) return -5;
     }
+    // last epilogue: lane bit sw_lane[s] trades places with column bit 1 + s
+    // (a warp shuffle in the kernel); the store-side index bits of the row
+    // and column bits follow the exchange
+    int32_t st_row[7], st_col[5];
+    tc_store_bits(P, st_row, st_col);
+    {
+      uint32_t seen = 0;
+      for (int s = 0; s < 3; ++s) {
+        const int l = P.sw_lane[s];
+        if (l < -1 || l > 4 || (l >= 0 && ((seen >> l) & 1u))) return -6;
+        if (l >= 0) seen |= 1u << l;
+      }
+    }
     // the kernel forms the epilogue offsets from one entry per column bit:
     // xnext and gcol must be linear (XOR of the next layout's offsets, sum of
     // the qubits' amplitude strides) in the bits of the column index
@@ -136,7 +150,7 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
         for (int i = 0; i < 5; ++i)
           if ((c >> i) & 1u) {
             if (j + 1 < m) x ^= P.u[j + 1].boff[P.u[j].fcol[i]];
-            g += 1ull << P.qt_out[P.u[j].fcol[i]];
+            g += 1ull << (j + 1 == m ? st_col[i] : P.qt_out[P.u[j].fcol[i]]);
           }
         if ((j + 1 < m && P.u[j].xnext[c] != x) || (j + 1 == m && P.u[j].gcol[c] != g)) return -4;
       }
@@ -192,12 +206,24 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
           for (int i = 0; i < 7; ++i)
             if ((r >> i) & 1u) {
               if (!last) ptn ^= P.u[j + 1].boff[P.u[j].frow[i]];
-              else pg |= 1ull << P.qt_out[P.u[j].frow[i]];
+              else pg |= 1ull << st_row[i];
             }
           const bool pair = !last && P.u[j + 1].boff[P.u[j].fcol[0]] == 4u;
           for (uint32_t c = 0; c < 32; ++c) {
-            double re = (D[r * 128 + 2 * c] + D[r * 128 + 64 + 2 * c]) * uinv;
-            double im = (D[r * 128 + 2 * c + 1] + D[r * 128 + 64 + 2 * c + 1]) * uinv;
+            // the thread of row r holds, in its register of column c, the
+            // element (rs, cs): after the lane exchanges of the last epilogue,
+            // row bit sw_lane[s] comes from c's bit 1 + s and vice versa
+            uint32_t rs = r, cs = c;
+            if (last)
+              for (int s = 0; s < 3; ++s) {
+                const int l = P.sw_lane[s];
+                if (l < 0) continue;
+                const uint32_t rb = (r >> l) & 1u, cb = (c >> (1 + s)) & 1u;
+                rs = (rs & ~(1u << l)) | (cb << l);
+                cs = (cs & ~(1u << (1 + s))) | (rb << (1 + s));
+              }
+            double re = (D[rs * 128 + 2 * cs] + D[rs * 128 + 64 + 2 * cs]) * uinv;
+            double im = (D[rs * 128 + 2 * cs + 1] + D[rs * 128 + 64 + 2 * cs + 1]) * uinv;
             if (split) {
               re = double(float(re));
               im = double(float(im));
@@ -232,6 +258,40 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
     stats[0] = int64_t(plan.passes.size());
     stats[1] = unitaries;
     stats[2] = int64_t(plan.stats.upload_bytes);
+  }
+  return int(plan.passes.size());
+}
+
+// Plan only: the 128-byte lines one warp store of each pass's last epilogue
+// touches (2^k, k = lane bits storing to index bits >= 4), summed over the
+// passes, with (out[0]) and without (out[1]) the lane exchanges, and the
+// exchanges made (out[2]).  Returns the number of passes or -1.
+extern "C" int emu_tc_store_lines(int n, const double* flat, int ngates, int64_t* out) {
+  std::vector<GateRec> gates(static_cast<size_t>(ngates));
+  for (int i = 0; i < ngates; ++i) {
+    const double* g = flat + size_t(i) * 40;
+    GateRec& r = gates[size_t(i)];
+    r.code = uint8_t(g[0]);
+    r.nq = uint8_t(gate_arity(r.code));
+    for (int j = 0; j < 3; ++j) r.q[j] = int(g[1 + j]);
+    for (int j = 0; j < 4; ++j) r.p[j] = g[4 + j];
+    for (int j = 0; j < 16; ++j) r.m[j] = cplx(g[8 + 2 * j], g[9 + 2 * j]);
+  }
+  TcPlan plan;
+  std::string err;
+  if (!build_tc_plan(lower_circuit(gates), n, &plan, &err)) return -1;
+  out[0] = out[1] = out[2] = 0;
+  for (const TcPassRec& P : plan.passes) {
+    int32_t st_row[7], st_col[5];
+    tc_store_bits(P, st_row, st_col);
+    int k = 0, k0 = 0;
+    for (int i = 0; i < 5; ++i) {
+      k += st_row[i] >= 4 ? 1 : 0;
+      k0 += P.qt_out[P.u[P.m - 1].frow[i]] >= 4 ? 1 : 0;
+    }
+    out[0] += int64_t(1) << k;
+    out[1] += int64_t(1) << k0;
+    for (int s = 0; s < 3; ++s) out[2] += P.sw_lane[s] >= 0 ? 1 : 0;
   }
   return int(plan.passes.size());
 }
