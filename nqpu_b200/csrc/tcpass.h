@@ -30,6 +30,7 @@ constexpr int kTcMaxUnitaries = 3;   // per pass (their B operands stay in share
 constexpr int kTcMinQubits = 12;
 constexpr int kTcLoadThreadBits = 7; // loading threads per tile engine: 128
 constexpr int kTcLoadStepBits = 4;   // 16-byte chunks per thread: 16
+constexpr int kTcMaxLaneSwaps = 3;  // last epilogue: lane exchanges with column bits 1..kTcMaxLaneSwaps
 // The unitaries are stored as 16 U (entries up to 16 in magnitude keep their
 // small entries clear of the FP16 subnormal range); epilogues divide by 16.
 constexpr float kTcUScale = 16.0f;

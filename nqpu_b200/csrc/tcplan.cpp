@@ -92,9 +92,9 @@ int lane_swaps(const int* frow, const int* fcol, const int* qt, int32_t* sw) {
   bool used[5] = {false, false, false, false, false};
   int cnt = 0;
   int order[3] = {1, 2, 3};  // column bits by their index bit, lowest first
-  std::sort(order, order + 3, [&](int a, int b) { return qt[fcol[a]] < qt[fcol[b]]; });
+  std::sort(order, order + kTcMaxLaneSwaps, [&](int a, int b) { return qt[fcol[a]] < qt[fcol[b]]; });
   for (int s = 0; s < 3; ++s) sw[s] = -1;
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < kTcMaxLaneSwaps; ++k) {
     const int cb = order[k];
     if (qt[fcol[cb]] > 3) continue;
     int best = -1;

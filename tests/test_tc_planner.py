@@ -128,3 +128,35 @@ def test_nonnormalised_input_state(emu):
     o.set_amplitudes(init)
     o.apply(gates)
     assert np.abs(got - o.amplitudes()).max() < 1e-12
+
+
+def store_lines(lib, n, gates):
+    lib.emu_tc_store_lines.restype = C.c_int
+    lib.emu_tc_store_lines.argtypes = [C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int64)]
+    flat = np.ascontiguousarray(circuits.flatten(gates))
+    out = (C.c_int64 * 3)()
+    npass = lib.emu_tc_store_lines(n, flat.ctypes.data_as(C.POINTER(C.c_double)), len(flat), out)
+    assert npass > 0
+    return out[0] / npass, out[1] / npass, out[2]
+
+
+@pytest.mark.parametrize("n,depth", [(26, 10), (30, 40)])
+def test_lane_exchanges_coalesce_the_last_epilogue_stores(emu, n, depth):
+    # a warp store of the last epilogue touches 2^k 128-byte lines (k lane bits
+    # on index bits >= 4); the lane exchanges bring the plan near the minimum
+    # of 4 (16-byte stores) / 2 (8-byte stores)
+    with_x, without_x, exchanges = store_lines(emu, n, circuits.brickwork(n, depth, seed=1))
+    assert exchanges > 0
+    assert with_x <= 4.0 and with_x < 0.5 * without_x, (with_x, without_x)
+
+
+@pytest.mark.parametrize("n,seed", [(14, 5), (15, 6)])
+def test_lane_exchanges_keep_fp64_parity(emu, n, seed):
+    # the emulator replays the kernel's register exchange: parity with the
+    # oracle on circuits whose plans make exchanges
+    gates = circuits.brickwork(n, 10, seed=seed)
+    assert store_lines(emu, n, gates)[2] > 0
+    got, _ = run_emu(emu, n, gates)
+    o = OracleState(n)
+    o.apply(gates)
+    assert np.abs(got - o.amplitudes()).max() < 1e-12
