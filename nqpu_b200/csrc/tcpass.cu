@@ -2,35 +2,39 @@
 // pass, each applied as a tcgen05 GEMM with split FP16 operands on a tile held
 // in shared memory (plan data and layouts in tcpass.h, planner in tcplan.cpp).
 //
-// Per pass, one persistent CTA per SM with four independent tile engines of
+// Per pass, one persistent CTA per SM with five independent tile engines of
 // four warps (one per TMEM lane quadrant).  An engine owns an operand buffer
 // (the tile as the 128 x 64 FP16 A operand: hi and lo planes, K-major,
 // 128-byte swizzle, 32 KB) and a 64-column TMEM accumulator, and runs its
 // tiles through:
 //   load     the tile's 32 KB (128 runs of 32 contiguous amplitudes) arrive
 //            by 16-byte cp.async as raw FP32 in the engine's own operand
-//            buffer; they are issued as soon as the previous tile's last MMAs
-//            are done, so they fly during that tile's last epilogue;
-//   split    each thread reads back its own 16 chunks, the engine meets at a
-//            barrier (the buffer is converted in place), then scales by s (a
-//            power of two, for the FP16 range) and the renormalisation
-//            factor, splits x = hi + lo into FP16 pairs and stores them in
-//            unitary 0's operand layout;
+//            buffer, at the plan's landing offsets (tcpass.h:
+//            tc_raw_offsets); they are issued as soon as the previous tile's
+//            last MMAs are done, so they fly during that tile's last epilogue;
+//   split    in two halves (load-step bit 3 = 0, 1), each landed in the
+//            slots that only its own outputs fill: each thread reads back its
+//            own 8 chunks of the half, the engine meets at a barrier (the
+//            buffer is converted in place), then scales by s (a power of two,
+//            for the FP16 range) and the renormalisation factor, splits
+//            x = hi + lo into FP16 pairs and stores them in unitary 0's
+//            operand layout (half the raw tile in registers at a time is what
+//            lets five engines run at 96 registers);
 //   unitary  one elected thread issues 12 MMAs (K = 16, N = 64) into the
 //            engine's 64-column accumulator: D = A_hi B_hi^T + A_hi B_lo^T +
 //            A_lo B_hi^T, B = the real embedding of 16 U, and commits them to
 //            the engine's mbarrier; one warp polls it (bounded) while the
 //            other three wait at the engine's named barrier;
-//   epilogue each thread drains its row (TMEM lane) of D, four 4-column
-//            parts per TMEM load wait, forms out = D / 16 and either splits
-//            it straight into the next unitary's operand layout, or, after
-//            the last unitary, stores out / s to HBM; there, up to three
+//   epilogue each thread drains its row (TMEM lane) of D, two 4-column parts
+//            per TMEM load wait, forms out = D / 16 and either splits it
+//            straight into the next unitary's operand layout, or, after the
+//            last unitary, stores out / s to HBM; there, up to two
 //            warp-shuffle exchanges of a lane bit with a column bit first put
 //            the state's low index bits on lanes, so a warp store covers
-//            whole 128-byte lines (3.4 lines per store on the 30-qubit
+//            whole 128-byte lines (3.75 lines per store on the 30-qubit
 //            brickwork instead of 9.9; 6-7 % of the circuit's time).
-// While one engine waits for its MMAs the other three run, so the tensor
-// pipe, shared memory and HBM overlap across four tiles.  The B operands of
+// While one engine waits for its MMAs the other four run, so the tensor
+// pipe, shared memory and HBM overlap across five tiles.  The B operands of
 // the pass's unitaries stay in shared memory for the launch.  The stores
 // follow the pass's store-side index bits (qt_out), which may place the tile's
 // qubits on other state index bits than it loaded them from (see tcpass.h).
@@ -59,10 +63,13 @@
 namespace nqpu {
 
 // An engine is one warp per TMEM lane quadrant (4 warps, 128 threads): each
-// thread drains whole rows, so 512 threads per CTA with up to 128 registers
-// each.  (Measured on the 30-qubit brickwork against 8-warp engines with two
-// warps per quadrant at 64 registers: 2-3.5 % faster.)
-constexpr int kTcEngines = 4;
+// thread drains whole rows, so 640 threads per CTA with up to 96 registers
+// each.  (Measured on the 30-qubit brickwork: 4-warp engines against 8-warp
+// ones with two warps per quadrant at 64 registers, 2-3.5 % faster; five
+// engines with the two-phase split against four with the whole raw tile in
+// registers, about 1 % faster — the split's second barrier costs 2.5 %, the
+// fifth engine gains 3.5 %.)
+constexpr int kTcEngines = 5;
 constexpr int kTcEngineWarps = 4;
 constexpr int kTcEngineThreads = 32 * kTcEngineWarps;
 constexpr int kTcThreads = kTcEngines * kTcEngineThreads;
@@ -77,9 +84,9 @@ constexpr int kTcParts = kTcCols / 4;                         // epilogue parts 
 // All three split products accumulate into one 64-column accumulator (12
 // MMAs of N = 64).  (Measured against A_hi [B_hi; B_lo]^T with N = 128 plus
 // A_lo B_hi^T into 128 columns summed in the epilogue: the same speed, half
-// the infidelity, half the TMEM loads; a fifth engine, which the 64-column
-// accumulators would allow, measured 1.5 % slower at 96 registers.)
-constexpr int kTcBatch = 4;                                   // parts per TMEM load wait
+// the infidelity, half the TMEM loads.)  Two parts per TMEM load wait keep
+// the five engines' drain within 96 registers.
+constexpr int kTcBatch = 2;                                   // parts per TMEM load wait
 constexpr uint32_t kTcAccCols = 64;                           // accumulator columns per engine
 static_assert(kTcEngines * kTcAccCols <= 512, "accumulators fit tensor memory");
 static_assert(kTcParts % kTcBatch == 0, "whole batches");
@@ -97,6 +104,7 @@ struct TcTables {
   uint32_t xcb[kTcMaxUnitaries][5];  // epilogue of unitary j: next-layout operand offset of column bit i
   uint64_t gcb[kTcMaxUnitaries][5];  // epilogue of the last unitary: amplitude offset of column bit i
   uint32_t sob[kTcStpBits];          // loader: operand offset (unitary 0's layout) of step bit s
+  uint32_t rsb[kTcStpBits];          // loader: raw landing offset of step bit s
   uint64_t sgb[kTcStpBits];          // loader: amplitude offset of step bit s
 };
 
@@ -211,6 +219,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   if (tid < kTcStpBits) {
     T->sob[tid] = P.u[0].boff[P.lt[kTcThrBits + tid]];
+    T->rsb[tid] = P.roff[P.lt[kTcThrBits + tid]];
     T->sgb[tid] = 1ull << P.qt[P.lt[kTcThrBits + tid]];
   }
   const uint32_t mbar_s = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar[0]));
@@ -264,11 +273,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   // ---- per-thread address parts ----
   // loader: thread bit b of et is tile bit lt[b], step bit s is tile bit
   // lt[kTcThrBits + s], and tile bit 0 is the pair inside each 16-byte load
-  uint32_t pol = 0;
+  uint32_t pol = 0, raw_t = 0;
   uint64_t pgl = 0;
   for (int b = 0; b < kTcThrBits; ++b)
     if ((et >> b) & 1) {
       pol ^= P.u[0].boff[P.lt[b]];
+      raw_t ^= P.roff[P.lt[b]];
       pgl |= 1ull << P.qt[P.lt[b]];
     }
   const uint32_t boff_h = P.u[0].boff[0];
@@ -330,9 +340,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
   };
   // raw FP32 chunks of `tile` into the engine's operand buffer by 16-byte
-  // cp.async: this thread's chunk of step i at raw_part + 16 i (threads of
-  // the engine); each thread reads back only its own chunks
-  const uint32_t raw_part = 16u * uint32_t(et);
+  // cp.async: this thread's chunk of step i at raw_t ^ (the step bits' raw
+  // offsets), in the 16-byte slots its own half of the split fills (the
+  // plan's landing offsets); each thread reads back only its own chunks
+  // (the step bits' entries are read from the shared tables where they are
+  // used: no registers held across the drain or the split)
+  auto raw_off = [&](int i) {
+    uint32_t r = raw_t;
+#pragma unroll
+    for (int b = 0; b < kTcStpBits; ++b)
+      if ((i >> b) & 1) r ^= T->rsb[b];
+    return r;
+  };
   auto issue_loads = [&](uint32_t tile) {
     const uint64_t tbn = tile_base_of(tile);
     const float4* src = reinterpret_cast<const float4*>(amp) + ((tbn + pgl) >> 1);
@@ -345,7 +364,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
       for (int b = 0; b < kTcStpBits; ++b)
         if ((i >> b) & 1) a += sgb[b];
-      cp_async16_s(ahi_s + raw_part + 16u * uint32_t(i * kTcEngineThreads), src + a);
+      cp_async16_s(ahi_s + raw_off(i), src + a);
     }
     cp_async_commit();
   };
@@ -359,14 +378,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint64_t tb = tile_base_of(tile);
     // ---- load, scale, split into unitary 0's operand ----
     {
-      float4 v[kTcLoadSteps];
       cp_async_wait0();
-#pragma unroll
-      for (int i = 0; i < kTcLoadSteps; ++i) v[i] = lds_v4(ahi_s + raw_part + 16u * uint32_t(i * kTcEngineThreads));
       uint32_t sob[kTcStpBits];
 #pragma unroll
       for (int b = 0; b < kTcStpBits; ++b) sob[b] = T->sob[b];
-      engine_sync(e);  // every raw chunk is in registers before the operand overwrites the buffer
       const float2 s2 = make_float2(scale_in, scale_in);
       // compile-time forms: 8-byte operand stores when the two amplitudes of
       // a chunk are adjacent columns, the input norm on the first pass only
@@ -374,19 +389,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         constexpr bool kPair = decltype(pair_c)::value;
         constexpr bool kNorm = decltype(norm_c)::value;
         float2 nin = make_float2(0.0f, 0.0f);  // FP32 partials over this thread's amplitudes, FP64 across tiles
+        // two halves (load-step bit 3 = 0, 1): each half's raw chunks sit in
+        // the slots that only its own outputs overwrite, so half the chunks
+        // are in registers at a time
 #pragma unroll
-        for (int i = 0; i < kTcLoadSteps; ++i) {
-          const float2 x0 = make_float2(v[i].x, v[i].y), x1 = make_float2(v[i].z, v[i].w);
-          if constexpr (kNorm) nin = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nin));
-          uint32_t o = pol;
+        for (int h = 0; h < 2; ++h) {
+          constexpr int kHalf = kTcLoadSteps / 2;
+          float4 v[kHalf];
 #pragma unroll
-          for (int b = 0; b < kTcStpBits; ++b)
-            if ((i >> b) & 1) o ^= sob[b];
-          if constexpr (kPair) {
-            put2(o, __fmul2_rn(x0, s2), __fmul2_rn(x1, s2));
-          } else {
-            put1(o, __fmul2_rn(x0, s2));
-            put1(o ^ boff_h, __fmul2_rn(x1, s2));
+          for (int ii = 0; ii < kHalf; ++ii) v[ii] = lds_v4(ahi_s + raw_off(ii + h * kHalf));
+          engine_sync(e);  // this half's raw chunks are in registers before its operand overwrites them
+#pragma unroll
+          for (int ii = 0; ii < kHalf; ++ii) {
+            const int i = ii + h * kHalf;
+            const float2 x0 = make_float2(v[ii].x, v[ii].y), x1 = make_float2(v[ii].z, v[ii].w);
+            if constexpr (kNorm) nin = __ffma2_rn(x1, x1, __ffma2_rn(x0, x0, nin));
+            uint32_t o = pol;
+#pragma unroll
+            for (int b = 0; b < kTcStpBits; ++b)
+              if ((i >> b) & 1) o ^= sob[b];
+            if constexpr (kPair) {
+              put2(o, __fmul2_rn(x0, s2), __fmul2_rn(x1, s2));
+            } else {
+              put1(o, __fmul2_rn(x0, s2));
+              put1(o ^ boff_h, __fmul2_rn(x1, s2));
+            }
           }
         }
         if constexpr (kNorm) norm_in += double(nin.x) + double(nin.y);

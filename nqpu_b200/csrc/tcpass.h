@@ -30,7 +30,7 @@ constexpr int kTcMaxUnitaries = 3;   // per pass (their B operands stay in share
 constexpr int kTcMinQubits = 12;
 constexpr int kTcLoadThreadBits = 7; // loading threads per tile engine: 128
 constexpr int kTcLoadStepBits = 4;   // 16-byte chunks per thread: 16
-constexpr int kTcMaxLaneSwaps = 3;  // last epilogue: lane exchanges with column bits 1..kTcMaxLaneSwaps
+constexpr int kTcMaxLaneSwaps = 2;  // last epilogue: lane exchanges with column bits 1..kTcMaxLaneSwaps
 // The unitaries are stored as 16 U (entries up to 16 in magnitude keep their
 // small entries clear of the FP16 subnormal range); epilogues divide by 16.
 constexpr float kTcUScale = 16.0f;
@@ -68,8 +68,44 @@ struct TcPassRec {
   // last epilogue: lane (row) bit exchanged with column bit 1 + s of the last
   // unitary by a shuffle before the HBM stores, or -1 (see tc_store_bits)
   int32_t sw_lane[3];
+  // loader: byte offset in the operand buffer where the 16-byte raw chunk of
+  // a load lands, as the XOR of one entry per tile bit (entry 0 unused: tile
+  // bit 0 is the pair inside a chunk); see tc_raw_offsets
+  uint32_t roff[kTcTileBits];
   TcUnitaryRec u[kTcMaxUnitaries];
 };
+
+// Raw landing offsets of a pass (TcPassRec::roff), given unitary 0's row
+// order (frow0) and the loader map (lt).  The copies of a tile land as raw
+// FP32 in the buffer that its FP16 hi / lo operand then overwrites, and the
+// split converts it in two halves (load-step bit 3 = 0, then 1), holding only
+// half the raw chunks in registers.  So the chunks of each half must land in
+// the 16-byte slots that only this half's own outputs fill.  In the swizzled
+// K-major layout, slot index bit i + 3 is the tile bit on row bit i (i >= 2)
+// and no other tile bit's slot offset carries it, so with the half bit lt[10]
+// on row bit hr (2..6) of unitary 0 the slots of half h are those with slot
+// bit hr + 3 = h.  The landing is a permutation of slot bits: loading-thread
+// bits 0..4 -> slot bits 0..4 (a warp's 32 chunks fill 512 contiguous bytes,
+// as the copies arrive), the half bit -> slot bit hr + 3, the other chunk bits
+// -> the remaining slot bits 5..10 in order.  Returns false when lt[10] is
+// not on row bits 2..6 (the planner's layout choice ensures it is).
+inline bool tc_raw_offsets(const int32_t* frow0, const int32_t* lt, uint32_t* roff) {
+  int hr = -1;
+  for (int i = 2; i < 7; ++i)
+    if (frow0[i] == lt[10]) hr = i;
+  if (hr < 0) return false;
+  const int fbit = hr + 3;
+  for (int b = 0; b < 12; ++b) roff[b] = 0;
+  for (int k = 0; k < 5; ++k) roff[lt[k]] = 16u << k;
+  int next = 5;
+  for (int k = 5; k < 10; ++k) {
+    if (next == fbit) ++next;
+    roff[lt[k]] = 16u << next;
+    ++next;
+  }
+  roff[lt[10]] = 16u << fbit;
+  return true;
+}
 
 // State index bit that row bit i / column bit i of the last unitary stores to.
 // The last epilogue holds D one row per lane; before its HBM stores, swap s

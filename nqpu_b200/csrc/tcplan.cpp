@@ -133,6 +133,10 @@ int layout_cost(const LayoutCfg& c, int m, const int* qt) {
   // tile bit 0 is column bit 0 of unitary 0, else two 4-byte stores
   if (c.fcol[0][0] == 0) cost += 64 * 2 * store_wavefronts(c.lt, boff[0], 8);
   else cost += 64 * 2 * 2 * store_wavefronts(c.lt, boff[0], 4);
+  // the split's half bit lt[10] must sit on row bits 2..6 of unitary 0 (the
+  // raw landing offsets need it; any other choice is invalid)
+  uint32_t roff[kTcTileBits];
+  if (!tc_raw_offsets(c.frow[0], c.lt, roff)) return 1 << 24;
   // epilogue: 4 warps x 32 columns (128 column-stores per tile, or 256
   // single ones), pairs of columns as 8-byte stores when
   // both layouts share column bit 0
@@ -537,6 +541,22 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     TcPassRec& P = out->passes[pi];
     choose_layouts(P);
     for (int j = 0; j < P.m; ++j) layout_offsets(P.u[j].frow, P.u[j].fcol, P.u[j].boff);
+    if (!tc_raw_offsets(P.u[0].frow, P.lt, P.roff)) {
+      // (the layout cost rules this out; kept valid in any case) a loader bit
+      // on row bits 2..6 of unitary 0 becomes the split's half bit: lt[0..2]
+      // hold at most three of those five tile bits, so lt[3..9] holds one
+      auto on_rows = [&](int tb) {
+        for (int i = 2; i < 7; ++i)
+          if (P.u[0].frow[i] == tb) return true;
+        return false;
+      };
+      for (int b = 9; b >= 3; --b)
+        if (on_rows(P.lt[b])) {
+          std::swap(P.lt[b], P.lt[10]);
+          break;
+        }
+      tc_raw_offsets(P.u[0].frow, P.lt, P.roff);
+    }
     lane_swaps(P.u[P.m - 1].frow, P.u[P.m - 1].fcol, P.qt_out, P.sw_lane);
     int32_t st_row[7], st_col[5];
     tc_store_bits(P, st_row, st_col);

@@ -64,7 +64,9 @@ extern "C" uint16_t emu_half_bits(float x) { return tc_half_bits(x); }
 // -1 plan failed, -2 operand slot written twice / misaligned, -3 amplitude
 // written twice or not at all, -4 a pairing condition does not hold,
 // -5 the loader's bit map is not a permutation with tile bits 1..3 first,
-// -6 the last epilogue's lane exchanges are not distinct lane bits 0..4.
+// -6 the last epilogue's lane exchanges are not distinct lane bits 0..4,
+// -7 the raw landing offsets are not a bijection onto 16-byte slots, or a
+// half of the two-phase split overwrites a raw chunk not yet read.
 extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, int split, int64_t* stats) {
   std::vector<GateRec> gates(static_cast<size_t>(ngates));
   for (int i = 0; i < ngates; ++i) {
@@ -156,6 +158,47 @@ extern "C" int emu_tc_run(int n, const double* flat, int ngates, double* state, 
       }
     const uint32_t boff_h = P.u[0].boff[0];
     const bool load_pair = boff_h == 4u;  // tile bit 0 is column bit 0 of unitary 0
+    {
+      // raw landing (kernel: raw_t ^ the step bits' T->rsb): chunk (thread gt,
+      // step i) lands at a 16-byte slot of the 32 KB operand buffer; the split
+      // reads the chunks of load-step bit 3 = 0, meets, writes their hi / lo
+      // outputs, then the same for bit 3 = 1.  No write may hit a slot whose
+      // raw chunk is still unread.
+      std::vector<int> owner(2048, -1);
+      std::vector<char> done(size_t(nthr * nstep), 0);
+      auto chunk_raw = [&](int gt, int i) {
+        uint32_t r = 0;
+        for (int b = 0; b < kTcLoadThreadBits; ++b)
+          if ((gt >> b) & 1) r ^= P.roff[P.lt[b]];
+        for (int b = 0; b < kTcLoadStepBits; ++b)
+          if ((i >> b) & 1) r ^= P.roff[P.lt[kTcLoadThreadBits + b]];
+        return r;
+      };
+      for (int gt = 0; gt < nthr; ++gt)
+        for (int i = 0; i < nstep; ++i) {
+          const uint32_t r = chunk_raw(gt, i);
+          if ((r & 15u) || r >= 32768u || owner[r >> 4] >= 0) return -7;
+          owner[r >> 4] = gt * nstep + i;
+        }
+      for (int h = 0; h < 2; ++h) {
+        for (int gt = 0; gt < nthr; ++gt)
+          for (int i = 0; i < nstep; ++i)
+            if ((i >> 3) == h) done[size_t(gt * nstep + i)] = 1;
+        for (int gt = 0; gt < nthr; ++gt) {
+          uint32_t pol = 0;
+          for (int b = 0; b < kTcLoadThreadBits; ++b)
+            if ((gt >> b) & 1) pol ^= P.u[0].boff[P.lt[b]];
+          for (int i = 0; i < nstep; ++i) {
+            if ((i >> 3) != h) continue;
+            const uint32_t o = pol ^ sol[size_t(i)];
+            for (uint32_t u : {o, o ^ boff_h, o + 16384u, (o ^ boff_h) + 16384u}) {
+              const int w = owner[u >> 4];
+              if (w >= 0 && !done[size_t(w)]) return -7;
+            }
+          }
+        }
+      }
+    }
     const bool store16 = P.qt_out[P.u[m - 1].fcol[0]] == 0;
     std::vector<int> amp_written(dim, 0);
     for (uint64_t tile = 0; tile < n_tiles; ++tile) {
