@@ -7,7 +7,7 @@
 // (the tile as the 128 x 64 FP16 A operand: hi and lo planes, K-major,
 // 128-byte swizzle, 32 KB) and a 64-column TMEM accumulator, and runs its
 // tiles through:
-//   load     the tile's 32 KB (128 runs of 32 contiguous amplitudes) arrive
+//   load     the tile's 32 KB (256 runs of 16 contiguous amplitudes) arrive
 //            by 16-byte cp.async as raw FP32 in the engine's own operand
 //            buffer, at the plan's landing offsets (tcpass.h:
 //            tc_raw_offsets); they are issued as soon as the previous tile's

@@ -4,8 +4,9 @@
 //
 // One HBM pass streams the complex64 state through the SMs once.  A tile is
 // the 2^12 amplitudes that agree on every qubit outside the pass's tile-qubit
-// set Q (12 qubits; tile bit b <-> qubit qt[b]; tile bits 0..4 are qubits 0..4,
-// so a tile is 128 runs of 32 contiguous amplitudes).  The pass applies up to
+// set Q (12 qubits; tile bit b <-> qubit qt[b]; tile bits 0..3 are qubits 0..3,
+// so a tile is 256 runs of 16 contiguous amplitudes: 128-byte lines).  The
+// pass applies up to
 // kTcMaxUnitaries fused unitaries, each a dense 32x32 matrix on 5 of the tile
 // qubits, in order.  For unitary j the tile is a 128 x 32 complex matrix: row
 // bits = the 7 other tile bits (frow[i] = tile bit of row bit i), column bits =
@@ -25,7 +26,7 @@
 namespace nqpu {
 
 constexpr int kTcTileBits = 12;
-constexpr int kTcLowBits = 5;        // tile bits 0..4 = qubits 0..4
+constexpr int kTcLowBits = 4;        // tile bits 0..3 = index bits 0..3 (the 128-byte runs)
 constexpr int kTcMaxUnitaries = 3;   // per pass (their B operands stay in shared memory)
 constexpr int kTcMinQubits = 12;
 constexpr int kTcLoadThreadBits = 7; // loading threads per tile engine: 128
@@ -56,7 +57,7 @@ struct TcUnitaryRec {
 
 struct TcPassRec {
   int32_t m;                     // unitaries in this pass (1..kTcMaxUnitaries)
-  int32_t qt[kTcTileBits];       // state index bit of tile bit b when the pass loads (0..4: bits 0..4)
+  int32_t qt[kTcTileBits];       // state index bit of tile bit b when the pass loads (0..3: bits 0..3)
   int32_t qt_out[kTcTileBits];   // state index bit of tile bit b when the pass stores (a permutation
                                  // of qt: the pass may move qubits between index bits, see TcPlan)
   int32_t n_out;                 // qubits outside Q (tile-id bits)
@@ -128,9 +129,9 @@ inline void tc_store_bits(const TcPassRec& P, int32_t* row_bits, int32_t* col_bi
 
 // Qubit placement: a pass may store its tile with its qubits on other state
 // index bits than it loaded them from (qt_out), so that the qubits the next
-// pass needs sit on index bits 0..4, which every tile must contain (they make
-// the 256-byte runs of its HBM accesses).  Placements are swaps of a qubit on
-// bits 0..4 with one elsewhere; the plan's last pass (or an added pass with an
+// pass needs sit on index bits 0..3, which every tile must contain (they make
+// the 128-byte runs of its HBM accesses).  Placements are swaps of a qubit on
+// bits 0..3 with one elsewhere; the plan's last pass (or an added pass with an
 // identity unitary) puts every qubit back on its own bit, so a run ends in
 // the natural order.
 struct TcPlan {

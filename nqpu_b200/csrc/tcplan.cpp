@@ -1,7 +1,7 @@
 // Host planner of the tensor-core pass mode (see tcpass.h for the plan data).
 //
 // Passes: ops are taken greedily in circuit order into the current pass while
-// the union of their qubits with qubits 0..4 stays within 12 (the tile); an op
+// the union of their qubits with qubits 0..3 stays within 12 (the tile); an op
 // may move ahead of an op left for a later pass only when the two share no
 // qubit (they commute), as in the tiled planner.  Within a pass the taken ops
 // are packed greedily, in order and under the same commutation rule, into
@@ -347,7 +347,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
   for (size_t i = 0; i < ops.size(); ++i) remaining[i] = int(i);
   // qubit placement: at[p] = qubit on state index bit p, pos[q] = index bit of
   // qubit q.  Invariant: every displaced qubit is one of a swap pair (l, X),
-  // l < 5 <= X: qubit X on bit l and qubit l on bit X.
+  // l < 4 <= X: qubit X on bit l and qubit l on bit X.
   std::vector<int> at(static_cast<size_t>(n)), pos(static_cast<size_t>(n));
   for (int q = 0; q < n; ++q) at[size_t(q)] = pos[size_t(q)] = q;
   auto low_qubits = [&]() {
@@ -361,7 +361,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     return true;
   };
   while (!remaining.empty() || !placed_home()) {
-    // ---- ops of the pass (the qubits on bits 0..4 are always in the tile) ----
+    // ---- ops of the pass (the qubits on bits 0..3 are always in the tile) ----
     uint64_t Q = low_qubits(), blocked = 0;
     std::vector<int> taken, rest;
     for (int idx : remaining) {
@@ -413,7 +413,7 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
       rest.swap(merged);
     }
     if (clusters.empty()) clusters.emplace_back(0, std::vector<int>());  // a placement-only pass: identity
-    // ---- the qubits the next pass wants on bits 0..4: the first qubits of
+    // ---- the qubits the next pass wants on bits 0..3: the first qubits of
     // the ops still to come (none left: the displaced low qubits, to go home) ----
     std::vector<int> want;
     {
@@ -433,25 +433,25 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
           if (at[size_t(l)] != l) want.push_back(l);
     }
     // fill the tile to 12 qubits: wanted qubits first (they can then be
-    // placed on bits 0..4 by this pass's stores), then the lowest unused
+    // placed on bits 0..3 by this pass's stores), then the lowest unused
     for (int q : want)
       if (popc(Q) < kTcTileBits) Q |= 1ull << q;
     for (int q = 0; q < n && popc(Q) < kTcTileBits; ++q) Q |= 1ull << q;
-    // ---- placement after the pass: wanted qubits onto bits 0..4 by swaps
+    // ---- placement after the pass: wanted qubits onto bits 0..3 by swaps
     // inside the tile (the tile's index bits are pos[Q]) ----
     std::vector<int> at_new = at, pos_new = pos;
     {
       auto in_tile = [&](int q) { return ((Q >> q) & 1ull) != 0; };
-      // at most 5 wanted qubits that are in the tile, in order of need
+      // at most kTcLowBits wanted qubits that are in the tile, in order of need
       std::vector<int> cand;
       for (int q : want)
         if (in_tile(q) && cand.size() < size_t(kTcLowBits)) cand.push_back(q);
       auto is_cand = [&](int q) { return std::find(cand.begin(), cand.end(), q) != cand.end(); };
-      bool fixed[kTcLowBits] = {false, false, false, false, false};
+      bool fixed[kTcLowBits] = {};
       for (int l = 0; l < kTcLowBits; ++l)
         if (is_cand(at_new[size_t(l)])) fixed[l] = true;  // already where it is wanted
       for (int y : cand) {
-        if (pos_new[size_t(y)] < kTcLowBits) continue;  // already on bits 0..4
+        if (pos_new[size_t(y)] < kTcLowBits) continue;  // already on bits 0..3
         if (y < kTcLowBits) {
           // a low qubit displaced to bit X: swap it home if bit y is free to change
           if (fixed[y]) continue;
@@ -493,8 +493,8 @@ bool build_tc_plan(const std::vector<Op>& ops, int n, TcPlan* out, std::string* 
     for (int s = 0; s < 3; ++s) P.sw_lane[s] = -1;
     std::array<int32_t, kTcTileBits> lq{};
     {
-      // tile bits in the order of their index bits when loaded (bits 0..4
-      // first: the 256-byte runs); the stores use the new placement
+      // tile bits in the order of their index bits when loaded (bits 0..3
+      // first: the 128-byte runs); the stores use the new placement
       int b = 0;
       for (int p = 0; p < n; ++p)
         if ((Q >> at[size_t(p)]) & 1ull) {
