@@ -191,7 +191,7 @@ def run_reference(args):
 # per pass), so the per-launch traffic is this figure times 2^n.
 DRAM_BYTES_PER_AMP = {
     "k_tile_pass": 15.14,  # 26q brickwork depth 8, two launches averaged
-    "k_tc_pass": 15.13,    # 26q brickwork depth 10, two launches averaged (537.0 MB read + 478.0 MB written)
+    "k_tc_pass": 15.12,    # 26q brickwork depth 10, two launches averaged (537.0 MB read + 477.4 MB written)
 }
 
 
