@@ -338,3 +338,53 @@ extern "C" int emu_tc_store_lines(int n, const double* flat, int ngates, int64_t
   }
   return int(plan.passes.size());
 }
+
+// The raw landing alone (tcpass.h: tc_raw_offsets), over `trials` seeded random
+// layouts of unitary 0 (row / column orders) and loader maps: for every valid
+// choice (half bit lt[10] on row bits 2..6), the 2048 chunks must land on
+// distinct 16-byte slots of the 32 KB buffer, and every chunk of half h must
+// land in a slot that only half h's hi / lo outputs fill.  Returns the number
+// of valid layouts checked, or -1 on the first violation.
+extern "C" int emu_tc_raw_landing(int trials, uint64_t seed) {
+  uint64_t s = seed | 1u;
+  auto rnd = [&](int k) {
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    return int(s % uint64_t(k));
+  };
+  int valid = 0;
+  for (int t = 0; t < trials; ++t) {
+    int perm[12];
+    for (int b = 0; b < 12; ++b) perm[b] = b;
+    for (int i = 11; i > 0; --i) std::swap(perm[i], perm[rnd(i + 1)]);
+    int32_t frow[7], fcol[5];
+    for (int i = 0; i < 7; ++i) frow[i] = perm[i];
+    for (int i = 0; i < 5; ++i) fcol[i] = perm[7 + i];
+    uint32_t boff[12];
+    for (int i = 0; i < 7; ++i) boff[frow[i]] = tc_sw128_off(1u << i, 0);
+    for (int i = 0; i < 5; ++i) boff[fcol[i]] = tc_sw128_off(0, 2u << i);
+    int32_t lt[11] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11};
+    for (int i = 10; i > 3; --i) std::swap(lt[i], lt[3 + rnd(i - 2)]);
+    uint32_t roff[12];
+    if (!tc_raw_offsets(frow, lt, roff)) continue;
+    ++valid;
+    std::vector<int> owner(2048, -1);
+    for (int c = 0; c < 2048; ++c) {  // chunk bits: loader bits 0..10 -> tile bits lt[.]
+      uint32_t r = 0;
+      for (int k = 0; k < 11; ++k)
+        if ((c >> k) & 1) r ^= roff[lt[k]];
+      if ((r & 15u) || r >= 32768u || owner[r >> 4] >= 0) return -1;
+      owner[r >> 4] = c;
+    }
+    for (int c = 0; c < 2048; ++c) {
+      const int h = (c >> 10) & 1;  // loader bit 10 = load-step bit 3, the half bit
+      uint32_t o = 0;               // hi offset of the chunk's first amplitude (tile bit 0 = 0)
+      for (int k = 0; k < 11; ++k)
+        if ((c >> k) & 1) o ^= boff[lt[k]];
+      for (uint32_t u : {o, o ^ boff[0], o + 16384u, (o ^ boff[0]) + 16384u})
+        if (((owner[u >> 4] >> 10) & 1) != h) return -1;
+    }
+  }
+  return valid;
+}

@@ -160,3 +160,12 @@ def test_lane_exchanges_keep_fp64_parity(emu, n, seed):
     o = OracleState(n)
     o.apply(gates)
     assert np.abs(got - o.amplitudes()).max() < 1e-12
+
+
+def test_raw_landing_is_a_half_preserving_bijection(emu):
+    # the two-phase split's landing offsets, on random layouts: distinct
+    # 16-byte slots, and each half's raw chunks only where its own outputs go
+    emu.emu_tc_raw_landing.restype = C.c_int
+    emu.emu_tc_raw_landing.argtypes = [C.c_int, C.c_uint64]
+    valid = emu.emu_tc_raw_landing(4000, 12345)
+    assert valid > 500, valid
